@@ -1,0 +1,264 @@
+/*
+ * mdn.h -- C ABI of the B200 (sm_100a) engine for the per-step hot path of
+ * MD_nucleation: effective-domain molecular dynamics of vapor nucleation
+ * around an ion (the "seed"), many independent replicas per GPU.
+ *
+ * The reference program drives one replica through `class MD`
+ * (src/md.hpp:9-114).  Its per-step work is `MD::verlet` (src/verlet.cpp:20-39)
+ * plus the pair-list rebuild `MD::make_pair` (src/pairList/pairlist.cpp:16-49)
+ * and the force plugins derived from `class Potential`
+ * (src/potential/basePotential.hpp:5-17), registered by `MD::setPotential`
+ * (src/initialization/setPotential.cpp:7-111).  This library replaces that
+ * step for a batch of replicas: a host keeps parsing, initial placement and
+ * output, hands the state over once through mdn_create / mdn_upload_state,
+ * and advances it with mdn_step.
+ *
+ * Conventions: every function returns an int status (MDN_OK = 0, negative =
+ * error) and never aborts; mdn_last_error() gives the message of the last
+ * failure on the calling thread.  Units are the reference's "real" units:
+ * Angstrom, fs, g/mol, kcal/mol, e.  All arrays are plain host pointers;
+ * nothing in this header depends on CUDA or torch types.  A handle is not
+ * re-entrant: one host thread drives one handle.
+ */
+#ifndef MDN_H
+#define MDN_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MDN_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+#define MDN_OK             0
+#define MDN_ERR_ARG       -1  /* bad argument or descriptor */
+#define MDN_ERR_CUDA      -2  /* a CUDA call failed */
+#define MDN_ERR_NO_DEVICE -3  /* no CUDA device (or the library was built without one) */
+#define MDN_ERR_CAPACITY  -4  /* a descriptor exceeds a compiled limit */
+#define MDN_ERR_REPLICA   -5  /* one or more replicas raised a status bit, see mdn_get_status */
+
+/* ---- per-replica status bits (mdn_get_status) ---------------------------- */
+#define MDN_ST_SLAB_OVERFLOW   0x0001 /* more in-domain gas molecules than the slab holds */
+#define MDN_ST_CORE_OVERFLOW   0x0002 /* more in-domain vapor atoms than the core holds */
+#define MDN_ST_LIST_OVERFLOW   0x0004 /* gas-ion / gas-vapor / gas-gas pair list full */
+#define MDN_ST_SHAKE_NOCONV    0x0008 /* SHAKE hit its iteration cap */
+#define MDN_ST_NONFINITE       0x0010 /* a non-finite force, position or velocity */
+#define MDN_ST_FIXED_OVERFLOW  0x0020 /* a force left the 64-bit fixed-point range */
+#define MDN_ST_EVENT_OVERFLOW  0x0040 /* vapor in/out event log full (events dropped) */
+
+/* ---- Interactions keywords (src/initialization/setCondition.cpp:186-228) - */
+#define MDN_I_GI           0x0001 /* gi LJ                     (PotentialGasIon)     */
+#define MDN_I_VI           0x0002 /* vi LJcoul                 (PotentialVaporIon)   */
+#define MDN_I_VV           0x0004 /* vv LJcoul                 (PotentialVaporVapor) */
+#define MDN_I_GV           0x0008 /* gv LJ                     (PotentialVaporGas)   */
+#define MDN_I_GG           0x0010 /* gg LJ, corrected form     (PotentialGasGas)     */
+#define MDN_I_AMBER        0x0020 /* ion AMBER                 (PotentialAMBER)      */
+#define MDN_I_BMH          0x0040 /* ion Born-Mayer-Huggins-NaCl (PotentialBorn)     */
+#define MDN_I_GAS_INTRA    0x0080 /* gas bonds                 (PotentialGasIntra)   */
+#define MDN_I_VAPOR_INTRA  0x0100 /* vapor bonds/angles/dihedrals (PotentialVaporIntra) */
+#define MDN_I_EFIELD       0x0200 /* uniform field on ion charges (PotentialEfield)  */
+#define MDN_I_SHAKE        0x1000 /* "SHAKE H": X-H bonds are constraints */
+
+/* ---- reference behaviours reproduced on request (mdn_options.quirks) ------
+ * Each bit reproduces one behaviour of the reference that a corrected
+ * implementation would change.  MDN_Q_ALL is the default, so that results
+ * match the reference; clearing a bit selects the corrected behaviour.     */
+#define MDN_Q_GV_GAS_COUNT   0x01 /* gv inner loop runs over the gas atom count
+                                     (src/potential/VaporGas.cpp:15)          */
+#define MDN_Q_GAS_ROT_ZY     0x02 /* gas insertion rotates (x, y, y), not (x, y, z)
+                                     (src/pairList/updateGasIn.cpp:85,92)     */
+#define MDN_Q_N2_ROT_VYVZ    0x04 /* N2 insertion spin puts v_rot on both y and z
+                                     (src/pairList/updateGasIn.cpp:69-78)     */
+#define MDN_Q_ENERGY_BUCKETS 0x08 /* vapor bond/angle energy -> Ugas, vapor dihedral
+                                     -> Uion (src/potential/compute_intra.cpp:82,124,194) */
+#define MDN_Q_SHAKE_NO_VCORR 0x10 /* SHAKE moves positions only, no velocity
+                                     correction (src/shake.cpp:6-92)          */
+#define MDN_Q_ALL            0x1F
+
+/* energy buckets, the order of `struct Potentials` (src/struct.hpp:29-38) */
+#define MDN_U_ION 0
+#define MDN_U_GAS 1
+#define MDN_U_VAP 2
+#define MDN_U_GI  3
+#define MDN_U_GG  4
+#define MDN_U_VG  5
+#define MDN_U_VI  6
+#define MDN_U_VV  7
+#define MDN_N_ENERGY 8
+
+/* gas kinds, MD::gastype after readCondFile (src/initialization/setCondition.cpp:48-113) */
+#define MDN_GAS_HE     1
+#define MDN_GAS_N2     2
+#define MDN_GAS_N2MONO 3
+#define MDN_GAS_AR     4
+
+/* thermostat modes for the relaxation phase (src/nvt.cpp) */
+#define MDN_NVT_OFF   0   /* MD::setNVE */
+#define MDN_NVT_SCALE 1   /* MD::velocity_scaling (target 300 K) */
+#define MDN_NVT_NH    2   /* MD::nosehoover_zeta / nosehoover_ion */
+
+/* One molecule kind: the ion, or the template of a gas or vapor molecule.
+ * Indices are 0-based; types index the replica's type tables.             */
+typedef struct mdn_topology {
+  int           n_atoms;
+  const int*    type;       /* [n_atoms] atom type                                  */
+  const double* charge;     /* [n_atoms] partial charge (e)                         */
+  const double* x;          /* [3*n_atoms] ion: coordinates; gas/vapor: template   */
+  int n_bonds;     const int* bonds;      /* [3*n] i, j, bond type               */
+  int n_rigid;     const int* rigid;      /* [3*n] i, j, bond type (SHAKE pairs) */
+  int n_angles;    const int* angles;     /* [4*n] i, j, k, angle type           */
+  int n_dihedrals; const int* dihedrals;  /* [5*n] i, j, k, l, dihedral type     */
+} mdn_topology;
+
+/* Everything one replica needs: the content of `Variables` after
+ * MD::MD (src/initialization/md.cpp:8-40), in flat arrays.               */
+typedef struct mdn_replica_desc {
+  /* type tables (Variables::atypes/btypes/ctypes/dtypes, src/variables.hpp:98-101) */
+  int n_atom_types;  const double* atom_mass; const double* atom_eps; const double* atom_sigma;
+  int n_bond_types;  const double* bond_coeff;     /* [2*n] K (kcal/mol/A^2), r0 (A)         */
+  int n_angle_types; const double* angle_coeff;    /* [2*n] K (kcal/mol/rad^2), theta0 (rad) */
+  int n_dihedral_types; const int* dihedral_multi; /* [n] terms per type (<= 3)              */
+  const double* dihedral_coeff;                    /* [15*n] per term: K, n, d(deg), cos d, sin d */
+  /* the ion (seed) */
+  mdn_topology  ion;
+  const double* ion_v;          /* [3*ion.n_atoms] initial velocities (A/fs)             */
+  const int*    ion_bmh_type;   /* [ion.n_atoms] Born-Mayer-Huggins row: 0 = Na, 1 = Cl  */
+  /* gas species */
+  mdn_topology  gas;
+  int           gas_kind;       /* MDN_GAS_*                                             */
+  double        gas_com_mass;   /* molecule mass dividing the centre of mass (vars->mass) */
+  double        gas_mb_mass;    /* kg per molecule for Maxwell-Boltzmann draws (pp->mgas) */
+  /* vapor species */
+  mdn_topology  vapor;
+  double        vapor_com_mass;
+  double        vapor_mb_mass;
+  /* molecules (centres of mass, reference order: gas 0..n_gas-1, then vapor) */
+  int n_gas;   const double* gas_x;   const double* gas_v;   /* [3*n_gas]   */
+  int n_vapor; const double* vapor_x; const double* vapor_v; /* [3*n_vapor] */
+  /* run parameters */
+  double dt;          /* fs                                          */
+  double temperature; /* K                                           */
+  double box;         /* cubic box edge d_size (A)                   */
+  double cutoff;      /* CUTOFF (A); lists use (CUTOFF+MARGIN)^2     */
+  double margin;      /* MARGIN (A)                                  */
+  double r_inter;     /* effective-domain radius Rinter (A), 100     */
+  double overlap;     /* taper shell width Overlap (A), 10           */
+  unsigned int interactions;        /* MDN_I_* bits */
+  int    nvt_mode;                  /* MDN_NVT_*    */
+  double nvt_temperature;           /* Nose-Hoover target (pp->Tnh_ion) */
+  double efield[3];                 /* Ecoeff for MDN_I_EFIELD */
+  unsigned long long seed;          /* counter-based RNG key of this replica */
+} mdn_replica_desc;
+
+typedef struct mdn_options {
+  unsigned int quirks;       /* MDN_Q_* bits to reproduce (default MDN_Q_ALL)          */
+  int force_mode;            /* 0: FP32 pair math, int64 fixed-point sums (default);
+                                1: FP64 pair math, int64 fixed-point sums            */
+  int cluster_size;          /* CTAs cooperating on one replica (1..8); 0 = automatic   */
+  int threads;               /* threads per CTA (128..1024, multiple of 32); 0 = 512    */
+  int steps_per_launch;      /* steps advanced per kernel launch; 0 = whole mdn_step    */
+  int use_graph;             /* capture repeated launches in a CUDA graph               */
+  double capacity_factor;    /* slab / list headroom over the expected counts (>= 1)   */
+  int device;                /* CUDA device ordinal                                     */
+} mdn_options;
+
+typedef struct mdn_handle mdn_handle;
+
+/* Sizes and counters of one replica. */
+typedef struct mdn_replica_info {
+  int n_ion, gas_atoms, vapor_atoms;   /* atoms in the ion / a gas / a vapor molecule */
+  int n_gas, n_vapor;                  /* molecules                                  */
+  int n_gas_in, n_vapor_in;            /* molecules inside the effective domain      */
+  int loop_pair, loop_update;          /* MD::loopPair, MD::loop_update              */
+  int n_rebuilds;
+  long long step;                      /* steps advanced since creation              */
+  int status;                          /* MDN_ST_* bits                              */
+  int gi_pairs, gv_pairs, gg_pairs;    /* current pair-list sizes                    */
+} mdn_replica_info;
+
+/* Full state of one replica in the reference's layout (Variables, src/variables.hpp).
+ * Molecule index 0 is the ion, 1..n_gas the gas, then the vapor (group[0..2]).
+ * Atom rows of molecules outside the effective domain are not used: download
+ * leaves them untouched and upload ignores them.                           */
+typedef struct mdn_state {
+  double* ion_x;   double* ion_v;   double* ion_f;     /* [3*n_ion]              */
+  double* mol_x;   double* mol_v;                      /* [3*(1+n_gas+n_vapor)]  */
+  unsigned char* region;                               /* [1+n_gas+n_vapor]      */
+  double* gas_ax;  double* gas_av;  double* gas_af;    /* [3*gas_atoms*n_gas]    */
+  double* vap_ax;  double* vap_av;  double* vap_af;    /* [3*vapor_atoms*n_vapor]*/
+  double* vap_w;                                       /* [vapor_atoms*n_vapor] taper weights */
+  int    loop_pair, loop_update;
+  double zeta;
+  double margin_length;
+} mdn_state;
+
+/* A vapor molecule that stayed in (kind 1) or left (kind 2) the domain at a
+ * rebuild: the rows MD::Ovin / MD::Ovout append (src/output/output.cpp:44-65). */
+typedef struct mdn_event {
+  int replica, molecule, kind, pad;
+  long long step;
+  double dx[3], dv[3];   /* relative to the ion centre of mass */
+} mdn_event;
+
+/* ---- lifecycle ------------------------------------------------------------ */
+int  mdn_abi_version(void);
+void mdn_default_options(mdn_options* opt);
+const char* mdn_last_error(void);
+int  mdn_device_count(int* n);
+
+/* Allocates device memory for n replicas, uploads them and performs the
+ * initial MD::make_pair (src/initialization/md.cpp:34): every molecule starts
+ * outside the domain, those within the sphere are inserted.                */
+int  mdn_create(const mdn_replica_desc* descs, int n_replicas, const mdn_options* opt,
+                mdn_handle** out);
+void mdn_destroy(mdn_handle* h);
+
+/* ---- stepping ------------------------------------------------------------- */
+/* Advances every replica by n_steps calls of MD::verlet, rebuilding the
+ * effective domain on the device whenever MD::check_pairlist would.
+ * energy_mode: 0 = no energies, 1 = energies of the last step (eflag on the
+ * last step, as MD::run sets it), 2 = energies summed over every step.   */
+int  mdn_step(mdn_handle* h, long long n_steps, int energy_mode);
+/* MD::make_pair for every replica now (used after re-centering). */
+int  mdn_make_pair(mdn_handle* h);
+/* Re-centres every replica on its ion (src/run.cpp:42-53).  compat = 1 keeps
+ * the reference's effect (only the ion centre entry is zeroed); compat = 0
+ * shifts every position.  Then calls MD::make_pair.                        */
+int  mdn_recenter(mdn_handle* h, int compat);
+/* Thermostat of one replica (replica < 0: all); MDN_NVT_OFF is MD::setNVE. */
+int  mdn_set_nvt(mdn_handle* h, int replica, int mode, double temperature);
+/* Recomputes forces (and energies) on the current positions without moving
+ * anything; term_mask selects MDN_I_* terms (0 = all enabled terms).      */
+int  mdn_compute_forces(mdn_handle* h, unsigned int term_mask);
+
+/* ---- results -------------------------------------------------------------- */
+int  mdn_energies(mdn_handle* h, double* U);          /* [8*n_replicas], MDN_U_* order */
+int  mdn_get_status(mdn_handle* h, int* status);      /* [n_replicas] MDN_ST_* bits    */
+int  mdn_clear_status(mdn_handle* h);
+int  mdn_replica_info_get(mdn_handle* h, int replica, mdn_replica_info* info);
+int  mdn_download_state(mdn_handle* h, int replica, mdn_state* s);
+int  mdn_upload_state(mdn_handle* h, int replica, const mdn_state* s);
+/* Pair lists as (molecule, partner) rows: kind 0 = gas-ion (partner = ion
+ * atom), 1 = gas-vapor (partner = vapor molecule index), 2 = gas-gas.
+ * Molecule indices are 0-based within the gas / vapor groups.             */
+int  mdn_pair_list(mdn_handle* h, int replica, int kind, int* pairs, int capacity, int* count);
+/* In-domain atoms for the OVITO dump (MD::export_dump_close,
+ * src/output/output.cpp:133-170), molecule order, ion first.            */
+int  mdn_in_domain(mdn_handle* h, int replica, int capacity, int* count,
+                   int* type, double* x, double* v);
+/* Drains the vapor in/out event log of every replica. */
+int  mdn_events(mdn_handle* h, mdn_event* ev, int capacity, int* count);
+/* Kinetic energies (MD Observer::computeProps, src/output/observer.cpp:5-36):
+ * out[4*r + 0..3] = Kion, Kgas, Kvap (kcal/mol) and Tion (K).             */
+int  mdn_kinetic(mdn_handle* h, double* out);
+
+/* ---- timing / tuning ------------------------------------------------------ */
+/* Device time (ms) of the last mdn_step, measured with CUDA events on the
+ * stream the kernels were launched on; kernel_launches = kernels issued.  */
+int  mdn_last_timing(mdn_handle* h, double* ms, long long* kernel_launches);
+int  mdn_set_launch(mdn_handle* h, int cluster_size, int threads, int steps_per_launch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MDN_H */

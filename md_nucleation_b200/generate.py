@@ -1,0 +1,482 @@
+"""Seeded synthetic systems of the shapes the benchmark configurations name.
+
+Every system is generated from one integer seed (0x4D444E55 + 1000*config +
+replica).  The species follow the reference's own gas table and file
+conventions: type tables are ordered ion, gas, vapor; angles are stored in
+radians; dihedral types hold three (K, n, d) terms as in readIonFile
+(src/initialization/readIonFile.cpp:85-104).
+
+  config 0  Na4Cl3(+1) cluster (Born-Mayer-Huggins), 20 methanol, 2,000 He,
+            1e5 Pa, 300 K, dt 1 fs, SHAKE on X-H bonds
+  config 1  150-atom +1 chain (AMBER), 100 methanol, 100,000 N2 (rigid), 1e5 Pa
+  config 2  batched replicas: gas in {He, Ar, N2, N2mono} with 5k-100k
+            molecules, vapor in {methanol, 3-site water} with 10-300
+            molecules, seed in {NaCl cluster, chain of 50-300 atoms}; the gas
+            pressure of each replica is solved so that the expected number of
+            in-domain atoms is drawn log-uniform in 500-20,000
+  config 4  1,000,000 N2, 1,000 rigid water, 500-atom +2 chain
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+from typing import List, Optional
+
+import numpy as np
+
+from . import abi
+from .system import (GAS_TABLE, KB, NW, R_INTER, OVERLAP, ReplicaSpec, Topology,
+                     box_from_pressure, mb_mass_kg, mb_sigma)
+
+SEED_BASE = 0x4D444E55
+V_SPHERE = 4.0 / 3.0 * math.pi * (R_INTER + OVERLAP) ** 3
+DEG = math.pi / 180.0
+
+
+def seed_of(config: int, replica: int = 0) -> int:
+    return SEED_BASE + 1000 * config + replica
+
+
+# --------------------------------------------------------------------------
+# molecule kinds: each returns a "species" dict with local type tables
+# --------------------------------------------------------------------------
+@dataclass
+class Species:
+    names: List[str]
+    mass: List[float]
+    eps: List[float]
+    sigma: List[float]
+    top: Topology            # type indices local to this species
+    bond_coeff: np.ndarray   # [nb,2]
+    angle_coeff: np.ndarray  # [na,2]
+    dih_multi: np.ndarray
+    dih_coeff: np.ndarray    # [nd,15]
+    h_types: tuple = ()      # local types that count as hydrogen for "SHAKE H"
+    bmh: Optional[np.ndarray] = None
+
+
+def _dih_row(terms):
+    """Three (K, n, d_deg) terms -> readIonFile's 15-column row."""
+    row = []
+    for k in range(3):
+        K, n, d = terms[k] if k < len(terms) else (0.0, 0.0, 0.0)
+        row += [K, n, d, math.cos(d * DEG), math.sin(d * DEG)]
+    return row
+
+
+def _rotmat(rng):
+    """Uniform random rotation (quaternion method)."""
+    q = rng.normal(size=4)
+    q /= np.linalg.norm(q)
+    a, b, c, d = q
+    return np.array([[a*a+b*b-c*c-d*d, 2*(b*c-a*d), 2*(b*d+a*c)],
+                     [2*(b*c+a*d), a*a-b*b+c*c-d*d, 2*(c*d-a*b)],
+                     [2*(b*d-a*c), 2*(c*d+a*b), a*a-b*b-c*c+d*d]])
+
+
+def _perp(u, rng):
+    """A unit vector perpendicular to u."""
+    u = u / np.linalg.norm(u)
+    for _ in range(100):
+        w = np.cross(u, rng.normal(size=3))
+        if np.linalg.norm(w) > 1e-3:
+            return w / np.linalg.norm(w)
+    raise RuntimeError("no perpendicular found")
+
+
+def _angle(a, b, c):
+    u, v = a - b, c - b
+    return math.acos(np.clip(np.dot(u, v) / np.linalg.norm(u) / np.linalg.norm(v), -1, 1))
+
+
+def methanol() -> Species:
+    """C, O, HO, 3 HC: bonds 1.43/0.96/1.09 A, angles 108-109.5 deg, one C-O
+    torsion of periodicity 3, charges C +0.145, O -0.683, HO +0.418, HC +0.04."""
+    bC, bO, bH = 1.43, 0.96, 1.09
+    C0 = np.zeros(3)
+    O = np.array([bC, 0.0, 0.0])
+    th = 108.5 * DEG
+    HO = O + bO * np.array([-math.cos(th), math.sin(th), 0.0])
+    hs = []
+    for phi in (60.0, 180.0, 300.0):
+        t, p = 109.5 * DEG, phi * DEG
+        hs.append(C0 + bH * np.array([math.cos(t), math.sin(t) * math.cos(p),
+                                      math.sin(t) * math.sin(p)]))
+    x = np.array([C0, O, HO] + hs)
+    x -= x.mean(axis=0)
+    types = [0, 1, 2, 3, 3, 3]
+    bonds = [[0, 1, 0], [1, 2, 1], [0, 3, 2], [0, 4, 2], [0, 5, 2]]
+    angles = []
+    ang_coeff = []
+    def add_angle(i, j, k, K):
+        angles.append([i, j, k, len(ang_coeff)])
+        ang_coeff.append([K, _angle(x[i], x[j], x[k])])
+    add_angle(0, 1, 2, 55.0)
+    for h in (3, 4, 5):
+        add_angle(h, 0, 1, 50.0)
+    add_angle(3, 0, 4, 35.0)
+    add_angle(3, 0, 5, 35.0)
+    add_angle(4, 0, 5, 35.0)
+    dihedrals = [[3, 0, 1, 2, 0], [4, 0, 1, 2, 0], [5, 0, 1, 2, 0]]
+    return Species(
+        names=["C", "O", "HO", "HC"], mass=[12.011, 15.999, 1.008, 1.008],
+        eps=[0.066, 0.170, 0.010, 0.030], sigma=[3.50, 3.12, 1.00, 2.50],
+        top=Topology(type=types, charge=[0.145, -0.683, 0.418, 0.04, 0.04, 0.04], x=x,
+                     bonds=bonds, angles=angles, dihedrals=dihedrals),
+        bond_coeff=np.array([[320.0, bC], [553.0, bO], [340.0, bH]]),
+        angle_coeff=np.array(ang_coeff),
+        dih_multi=np.array([1], np.int32), dih_coeff=np.array([_dih_row([(0.18, 3, 0.0)])]),
+        h_types=(2, 3))
+
+
+def water() -> Species:
+    """3-site water, O -0.834 e, H +0.417 e (TIP3P geometry); the O-H and H-H
+    distances are bonds so that "SHAKE H" makes the molecule rigid."""
+    r, th = 0.9572, 104.52 * DEG
+    O = np.zeros(3)
+    H1 = r * np.array([math.sin(th / 2), math.cos(th / 2), 0.0])
+    H2 = r * np.array([-math.sin(th / 2), math.cos(th / 2), 0.0])
+    x = np.array([O, H1, H2])
+    x -= x.mean(axis=0)
+    hh = float(np.linalg.norm(H1 - H2))
+    return Species(
+        names=["OW", "HW"], mass=[15.999, 1.008], eps=[0.1521, 0.010], sigma=[3.1507, 1.0],
+        top=Topology(type=[0, 1, 1], charge=[-0.834, 0.417, 0.417], x=x,
+                     bonds=[[0, 1, 0], [0, 2, 0], [1, 2, 1]], angles=[[1, 0, 2, 0]]),
+        bond_coeff=np.array([[450.0, r], [0.0, hh]]),
+        angle_coeff=np.array([[55.0, th]]),
+        dih_multi=np.zeros(0, np.int32), dih_coeff=np.zeros((0, 15)),
+        h_types=(1,))
+
+
+def nacl_cluster() -> Species:
+    """Na4Cl3(+1): a 2x2x2 rock-salt cube (a = 2.82 A) missing one Cl corner.
+    Types: 0 = Na, 1 = Cl, which are also the Born-Mayer-Huggins rows."""
+    a = 2.82
+    xs, ts = [], []
+    for i in (0, 1):
+        for j in (0, 1):
+            for k in (0, 1):
+                if (i + j + k) % 2 == 0:
+                    xs.append([i * a, j * a, k * a]); ts.append(0)
+                elif (i, j, k) != (1, 1, 1):
+                    xs.append([i * a, j * a, k * a]); ts.append(1)
+    x = np.array(xs, float)
+    q = [1.0 if t == 0 else -1.0 for t in ts]
+    return Species(
+        names=["Na", "Cl"], mass=[22.99, 35.45], eps=[0.10, 0.10], sigma=[2.35, 4.40],
+        top=Topology(type=ts, charge=q, x=x),
+        bond_coeff=np.zeros((0, 2)), angle_coeff=np.zeros((0, 2)),
+        dih_multi=np.zeros(0, np.int32), dih_coeff=np.zeros((0, 15)),
+        bmh=np.array(ts, np.int32))
+
+
+def chain(n_atoms: int, charge: float, rng: np.random.Generator) -> Species:
+    """A +q peptide-like chain: a self-avoiding heavy-atom backbone (bonds
+    1.33-1.53 A, angles 110-120 deg, torsions of periodicity 1-3 with barriers
+    0-2 kcal/mol) carrying two hydrogens per heavy atom at 1.0-1.09 A; charges
+    N(0, 0.3 e) shifted to the net charge; LJ sigma 2.5-3.5 A, eps 0.02-0.2."""
+    n_heavy = max(3, n_atoms // 3)
+    n_h = n_atoms - n_heavy
+    n_heavy_types = 6
+    # backbone, grown as a self-avoiding walk
+    for _attempt in range(200):
+        bb = [np.zeros(3)]
+        bl = rng.uniform(1.33, 1.53, n_heavy)
+        ok = True
+        for i in range(1, n_heavy):
+            for _try in range(200):
+                if i == 1:
+                    d = rng.normal(size=3); d /= np.linalg.norm(d)
+                else:
+                    prev = bb[-1] - bb[-2]; prev /= np.linalg.norm(prev)
+                    th = rng.uniform(110, 120) * DEG
+                    perp = np.cross(prev, rng.normal(size=3)); perp /= np.linalg.norm(perp)
+                    d = math.cos(math.pi - th) * prev + math.sin(math.pi - th) * perp
+                cand = bb[-1] + bl[i] * d
+                if all(np.linalg.norm(cand - p) > 3.0 for p in bb[:-2]):
+                    bb.append(cand); break
+            else:
+                ok = False; break
+        if ok:
+            break
+    bb = np.array(bb)
+    # hydrogens: distributed over heavy atoms, placed off the backbone
+    per = np.full(n_heavy, n_h // n_heavy); per[: n_h % n_heavy] += 1
+    xs = list(bb)
+    types = list(rng.integers(0, n_heavy_types, n_heavy))
+    hpos, hpar = [], []
+    for i in range(n_heavy):
+        nb = [j for j in (i - 1, i + 1) if 0 <= j < n_heavy]
+        u = -sum((bb[j] - bb[i]) / np.linalg.norm(bb[j] - bb[i]) for j in nb)
+        if np.linalg.norm(u) < 1e-3:
+            u = _perp(bb[nb[0]] - bb[i], rng)
+        u /= np.linalg.norm(u)
+        w = _perp(u, rng)
+        for h in range(per[i]):
+            ang = 2 * math.pi * h / max(per[i], 1)
+            v = w * math.cos(ang) + np.cross(u, w) * math.sin(ang)
+            d = math.cos(54.75 * DEG) * u + math.sin(54.75 * DEG) * v
+            hpos.append(bb[i] + rng.uniform(1.0, 1.09) * d)
+            hpar.append(i)
+    xs = np.array(xs + hpos)
+    types = types + [n_heavy_types] * n_h
+    n = len(xs)
+    # bonded topology: one bond type / angle type / dihedral type per term,
+    # equilibrium values taken from the generated geometry
+    bonds, bond_coeff = [], []
+    def add_bond(i, j, K):
+        bonds.append([i, j, len(bond_coeff)])
+        bond_coeff.append([K, float(np.linalg.norm(xs[i] - xs[j]))])
+    for i in range(n_heavy - 1):
+        add_bond(i, i + 1, rng.uniform(250, 400))
+    for h, p in enumerate(hpar):
+        add_bond(p, n_heavy + h, 340.0)
+    angles, angle_coeff = [], []
+    def add_angle(i, j, k, K):
+        angles.append([i, j, k, len(angle_coeff)])
+        angle_coeff.append([K, _angle(xs[i], xs[j], xs[k])])
+    for i in range(1, n_heavy - 1):
+        add_angle(i - 1, i, i + 1, rng.uniform(40, 70))
+    hs_of = [[] for _ in range(n_heavy)]
+    for h, p in enumerate(hpar):
+        hs_of[p].append(n_heavy + h)
+    for i in range(n_heavy):
+        for hh in hs_of[i]:
+            for j in (i - 1, i + 1):
+                if 0 <= j < n_heavy:
+                    add_angle(hh, i, j, 50.0)
+        for a in range(len(hs_of[i])):
+            for b in range(a + 1, len(hs_of[i])):
+                add_angle(hs_of[i][a], i, hs_of[i][b], 35.0)
+    dihedrals, dih_multi, dih_coeff = [], [], []
+    for i in range(n_heavy - 3):
+        dihedrals.append([i, i + 1, i + 2, i + 3, len(dih_multi)])
+        nt = int(rng.integers(1, 3))
+        terms = [(rng.uniform(0, 2), int(rng.integers(1, 4)), float(rng.choice([0.0, 180.0])))
+                 for _ in range(nt)]
+        dih_multi.append(nt)
+        dih_coeff.append(_dih_row(terms))
+    for i in range(n_heavy - 2):
+        for hh in hs_of[i]:
+            dihedrals.append([hh, i, i + 1, i + 2, len(dih_multi)])
+            dih_multi.append(1)
+            dih_coeff.append(_dih_row([(rng.uniform(0, 0.5), 3, 0.0)]))
+    q = rng.normal(0, 0.3, n)
+    q += (charge - q.sum()) / n
+    xs -= xs.mean(axis=0)
+    return Species(
+        names=[f"X{k}" for k in range(n_heavy_types)] + ["H"],
+        mass=list(rng.choice([12.011, 14.007, 15.999], n_heavy_types)) + [1.008],
+        eps=list(rng.uniform(0.02, 0.2, n_heavy_types)) + [0.02],
+        sigma=list(rng.uniform(2.5, 3.5, n_heavy_types)) + [2.5],
+        top=Topology(type=types, charge=q, x=xs, bonds=bonds, angles=angles, dihedrals=dihedrals),
+        bond_coeff=np.array(bond_coeff), angle_coeff=np.array(angle_coeff),
+        dih_multi=np.array(dih_multi, np.int32), dih_coeff=np.array(dih_coeff),
+        h_types=(n_heavy_types,))
+
+
+def gas_species(name: str, rigid: bool = False) -> Species:
+    g = GAS_TABLE[name]
+    na = len(g["x"])
+    bonds = [[0, 1, 0]] if g["bond"] else []
+    return Species(names=[name], mass=[g["mass"]], eps=[g["eps"]], sigma=[g["sigma"]],
+                   top=Topology(type=[0] * na, charge=[0.0] * na, x=g["x"],
+                                bonds=[] if rigid else bonds, rigid=bonds if rigid else []),
+                   bond_coeff=np.array([g["bond"]]) if g["bond"] else np.zeros((0, 2)),
+                   angle_coeff=np.zeros((0, 2)), dih_multi=np.zeros(0, np.int32),
+                   dih_coeff=np.zeros((0, 15)))
+
+
+def _split_rigid(sp: Species, shake_h: bool):
+    """readIonFile/readVaporFile: with "SHAKE H", bonds touching an H type go to
+    rigid_pairs (src/initialization/readIonFile.cpp:131-137)."""
+    if not shake_h or len(sp.top.bonds) == 0:
+        return sp.top.bonds, sp.top.rigid
+    keep, rig = [], list(sp.top.rigid)
+    for b in sp.top.bonds:
+        if sp.top.type[b[0]] in sp.h_types or sp.top.type[b[1]] in sp.h_types:
+            rig.append(b)
+        else:
+            keep.append(b)
+    return np.array(keep, np.int32).reshape(-1, 3), np.array(rig, np.int32).reshape(-1, 3)
+
+
+# --------------------------------------------------------------------------
+# assembling a replica
+# --------------------------------------------------------------------------
+def assemble(ion: Species, gas: Species, vap: Species, *, gas_name: str, n_gas: int,
+             n_vap: int, T: float, p: float, dt: float, interactions: int, seed: int,
+             shake_h: bool, rng: np.random.Generator, nvt_mode=abi.NVT_OFF,
+             min_dist: float = 10.0, box: Optional[float] = None, label: str = "") -> ReplicaSpec:
+    """Concatenates the species' tables (ion, gas, vapor order), places the
+    molecules uniformly in the cube and draws Maxwell-Boltzmann velocities."""
+    offs_t, offs_b, offs_a, offs_d = [0], [0], [0], [0]
+    mass, eps, sig, names = [], [], [], []
+    bc, ac, dm, dc = [], [], [], []
+    tops = []
+    for sp in (ion, gas, vap):
+        t0, b0, a0, d0 = len(mass), len(bc), len(ac), len(dm)
+        mass += list(sp.mass); eps += list(sp.eps); sig += list(sp.sigma); names += list(sp.names)
+        bc += [list(r) for r in sp.bond_coeff]; ac += [list(r) for r in sp.angle_coeff]
+        dm += list(sp.dih_multi); dc += [list(r) for r in sp.dih_coeff]
+        bonds, rigid = _split_rigid(sp, shake_h)
+        top = Topology(type=np.asarray(sp.top.type) + t0, charge=sp.top.charge, x=sp.top.x,
+                       bonds=_shift(bonds, 3, 2, b0), rigid=_shift(rigid, 3, 2, b0),
+                       angles=_shift(sp.top.angles, 4, 3, a0),
+                       dihedrals=_shift(sp.top.dihedrals, 5, 4, d0))
+        tops.append(top)
+    ion_top, gas_top, vap_top = tops
+    if box is None:
+        box = box_from_pressure(n_gas, T, p)
+    # ion: uniform random orientation, MB velocities per atom
+    R = _rotmat(rng)
+    ion_top.x = np.ascontiguousarray(ion_top.x @ R.T)
+    m_ion = np.array([mass[t] for t in ion_top.type])
+    ion_v = rng.normal(size=(ion_top.n, 3)) * mb_sigma(T, m_ion[:, None] * 1e-3 / NW)
+    # vapor then gas centres, uniform in the cube, kept min_dist from the ion
+    # atoms and from the vapor already placed
+    half = box / 2
+    ion_r = np.linalg.norm(ion_top.x, axis=1).max() if ion_top.n else 0.0
+    if not np.all(np.isfinite(ion_top.x)):
+        raise RuntimeError("non-finite ion coordinates")
+    vx = []
+    tries = 0
+    while len(vx) < n_vap:
+        tries += 1
+        if tries > 1000 * (n_vap + 10):
+            raise RuntimeError("vapor placement did not converge")
+        c = rng.uniform(-half, half, 3)
+        if np.linalg.norm(c) < ion_r + min_dist:
+            continue
+        if vx and np.min(np.linalg.norm(np.array(vx) - c, axis=1)) < min_dist:
+            continue
+        vx.append(c)
+    vx = np.array(vx).reshape(-1, 3)
+    gx = np.empty((0, 3))
+    rounds = 0
+    while len(gx) < n_gas:
+        rounds += 1
+        if rounds > 200:
+            raise RuntimeError("gas placement did not converge")
+        c = rng.uniform(-half, half, (2 * (n_gas - len(gx)) + 16, 3))
+        ok = np.linalg.norm(c, axis=1) >= ion_r + min_dist
+        if len(vx):
+            for b in range(0, len(c), 4096):
+                d = np.linalg.norm(c[b:b + 4096, None, :] - vx[None], axis=2).min(axis=1)
+                ok[b:b + 4096] &= d >= min_dist
+        gx = np.concatenate([gx, c[ok]])[:n_gas]
+    g = GAS_TABLE[gas_name]
+    gas_m = mb_mass_kg(g["mol_mass"])
+    vap_com = float(sum(mass[t] for t in vap_top.type))
+    vap_m = mb_mass_kg(vap_com)
+    gv = rng.normal(size=(n_gas, 3)) * mb_sigma(T, gas_m)
+    vv = rng.normal(size=(n_vap, 3)) * mb_sigma(T, vap_m)
+    bmh = ion.bmh if ion.bmh is not None else np.zeros(ion_top.n, np.int32)
+    return ReplicaSpec(
+        atom_mass=mass, atom_eps=eps, atom_sigma=sig, atom_name=names,
+        bond_coeff=np.array(bc).reshape(-1, 2), angle_coeff=np.array(ac).reshape(-1, 2),
+        dihedral_multi=np.array(dm, np.int32), dihedral_coeff=np.array(dc).reshape(-1, 15),
+        ion=ion_top, ion_v=ion_v, ion_bmh_type=bmh,
+        gas=gas_top, gas_kind=g["kind"], gas_com_mass=g["mol_mass"], gas_mb_mass=gas_m,
+        vapor=vap_top, vapor_com_mass=vap_com, vapor_mb_mass=vap_m,
+        gas_x=gx, gas_v=gv, vapor_x=vx, vapor_v=vv,
+        dt=dt, temperature=T, box=box, interactions=interactions, nvt_mode=nvt_mode,
+        seed=seed, pressure=p, label=label)
+
+
+def _shift(arr, width, col, off):
+    a = np.array(arr, np.int32).reshape(-1, width).copy()
+    if len(a):
+        a[:, col] += off
+    return a
+
+
+BASE_TERMS = abi.I_GI | abi.I_GV | abi.I_VI | abi.I_VV | abi.I_GAS_INTRA | abi.I_VAPOR_INTRA
+
+
+def config0(replica: int = 0, n_gas: int = 2000, n_vap: int = 20) -> ReplicaSpec:
+    rng = np.random.default_rng(seed_of(0, replica))
+    return assemble(nacl_cluster(), gas_species("He"), methanol(), gas_name="He", n_gas=n_gas,
+                    n_vap=n_vap, T=300.0, p=1e5, dt=1.0,
+                    interactions=BASE_TERMS | abi.I_BMH | abi.I_SHAKE,
+                    seed=seed_of(0, replica), shake_h=True, rng=rng, label="config0")
+
+
+def config1(replica: int = 0, n_gas: int = 100_000, n_vap: int = 100, chain_atoms: int = 150,
+            rigid_n2: bool = True) -> ReplicaSpec:
+    rng = np.random.default_rng(seed_of(1, replica))
+    ion = chain(chain_atoms, 1.0, rng)
+    return assemble(ion, gas_species("N2", rigid=rigid_n2), methanol(), gas_name="N2",
+                    n_gas=n_gas, n_vap=n_vap, T=300.0, p=1e5, dt=1.0,
+                    interactions=BASE_TERMS | abi.I_AMBER | abi.I_SHAKE,
+                    seed=seed_of(1, replica), shake_h=True, rng=rng, label="config1")
+
+
+def config2_replica(replica: int, scale: float = 1.0) -> ReplicaSpec:
+    """One replica of the batched configuration.  scale < 1 shrinks the
+    molecule counts (tests use it); the density stays what the draw gives."""
+    seed = seed_of(2, replica)
+    rng = np.random.default_rng(seed)
+    gas_name = ["He", "Ar", "N2", "N2monoatomic"][int(rng.integers(0, 4))]
+    n_gas = int(round(math.exp(rng.uniform(math.log(5000), math.log(100_000))) * scale))
+    use_water = bool(rng.integers(0, 2))
+    n_vap = max(1, int(round(rng.uniform(10, 300) * scale)))
+    target = math.exp(rng.uniform(math.log(500), math.log(20_000))) * scale
+    if rng.integers(0, 2) == 0:
+        ion = nacl_cluster()
+        terms = BASE_TERMS | abi.I_BMH
+    else:
+        ion = chain(int(rng.integers(50, 301)), 1.0, rng)
+        terms = BASE_TERMS | abi.I_AMBER
+    vap = water() if use_water else methanol()
+    gas = gas_species(gas_name)
+    a_g = gas.top.n
+    T = 300.0
+    # in-domain gas molecules wanted -> number density -> box and pressure
+    gas_atoms_in = max(target - ion.top.n, 50.0)
+    n_dens = gas_atoms_in / a_g / V_SPHERE
+    box = (n_gas / n_dens) ** (1 / 3)
+    min_box = 2.2 * (R_INTER + OVERLAP)
+    if box < min_box:  # keep the sphere inside the periodic cell
+        n_gas = int(math.ceil(n_dens * min_box ** 3))
+        box = (n_gas / n_dens) ** (1 / 3)
+    p = n_dens * 1e30 * KB * T
+    spacing = n_dens ** (-1 / 3)
+    return assemble(ion, gas, vap, gas_name=gas_name, n_gas=n_gas, n_vap=n_vap, T=T, p=p,
+                    dt=1.0, interactions=terms | abi.I_SHAKE, seed=seed, shake_h=True, rng=rng,
+                    min_dist=min(10.0, 0.5 * spacing), box=box, label=f"config2[{replica}]")
+
+
+def config2(n_replicas: int = 256, scale: float = 1.0) -> List[ReplicaSpec]:
+    return [config2_replica(r, scale) for r in range(n_replicas)]
+
+
+def config4_replica(replica: int = 0, n_gas: int = 1_000_000, n_vap: int = 1000) -> ReplicaSpec:
+    rng = np.random.default_rng(seed_of(4, replica))
+    ion = chain(500, 2.0, rng)
+    return assemble(ion, gas_species("N2"), water(), gas_name="N2", n_gas=n_gas, n_vap=n_vap,
+                    T=300.0, p=1e5, dt=1.0,
+                    interactions=BASE_TERMS | abi.I_AMBER | abi.I_SHAKE,
+                    seed=seed_of(4, replica), shake_h=True, rng=rng, label="config4")
+
+
+def small_system(seed: int = 7, gas: str = "N2", vapor: str = "methanol", ion: str = "nacl",
+                 n_gas: int = 400, n_vap: int = 12, box: float = 260.0, interactions=None,
+                 shake_h: bool = False, rigid_gas: bool = False, chain_atoms: int = 30,
+                 nvt_mode=abi.NVT_OFF, dt: float = 1.0) -> ReplicaSpec:
+    """A small replica for parity tests: a dense gas in a small box so that
+    the sphere holds many molecules."""
+    rng = np.random.default_rng(seed)
+    ion_sp = nacl_cluster() if ion == "nacl" else chain(chain_atoms, 1.0, rng)
+    vap_sp = methanol() if vapor == "methanol" else water()
+    if interactions is None:
+        interactions = BASE_TERMS | (abi.I_BMH if ion == "nacl" else abi.I_AMBER)
+        if shake_h:
+            interactions |= abi.I_SHAKE
+    n_dens = n_gas / box ** 3
+    p = n_dens * 1e30 * KB * 300.0
+    return assemble(ion_sp, gas_species(gas, rigid=rigid_gas), vap_sp, gas_name=gas,
+                    n_gas=n_gas, n_vap=n_vap, T=300.0, p=p, dt=dt, interactions=interactions,
+                    seed=seed, shake_h=shake_h, rng=rng, nvt_mode=nvt_mode,
+                    min_dist=min(10.0, 0.5 * n_dens ** (-1 / 3)), box=box, label="small")
