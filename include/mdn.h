@@ -73,7 +73,9 @@ extern "C" {
                                      -> Uion (src/potential/compute_intra.cpp:82,124,194) */
 #define MDN_Q_SHAKE_NO_VCORR 0x10 /* SHAKE moves positions only, no velocity
                                      correction (src/shake.cpp:6-92)          */
-#define MDN_Q_ALL            0x1F
+#define MDN_Q_ALL            0x0F /* MDN_Q_SHAKE_NO_VCORR is opt-in: the reference never
+                                     calls its SHAKE (src/verlet.cpp:24), and the
+                                     position-only form heats the system */
 
 /* energy buckets, the order of `struct Potentials` (src/struct.hpp:29-38) */
 #define MDN_U_ION 0

@@ -34,7 +34,7 @@ Q_GAS_ROT_ZY = 0x02
 Q_N2_ROT_VYVZ = 0x04
 Q_ENERGY_BUCKETS = 0x08
 Q_SHAKE_NO_VCORR = 0x10
-Q_ALL = 0x1F
+Q_ALL = 0x0F  # Q_SHAKE_NO_VCORR is opt-in
 
 U_ION, U_GAS, U_VAP, U_GI, U_GG, U_VG, U_VI, U_VV = range(8)
 ENERGY_NAMES = ("Uion", "Ugas", "Uvap", "Ugi", "Ugg", "Uvg", "Uvi", "Uvv")

@@ -1,0 +1,64 @@
+"""Builds the engine library in-tree: md_nucleation_b200/lib/libmdn.so.
+
+nvcc compiles the CUDA sources for sm_100a only.  --fmad=false keeps FP64
+expressions rounding like the reference's x86 build; the FP32 pair kernels
+request fused multiply-adds explicitly with fmaf().
+"""
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB_DIR = os.path.join(HERE, "lib")
+LIB = os.path.join(LIB_DIR, "libmdn.so")
+SOURCES = ["advance.cu", "engine.cu"]
+HEADERS = ["mdn_types.h", "device_util.cuh"]
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-O3", "-lineinfo", "--fmad=false", "-std=c++17",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+]
+
+
+def nvcc():
+    for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if c and os.path.exists(c):
+            return c
+    raise RuntimeError("nvcc not found")
+
+
+def _stale():
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = [os.path.join(CSRC, s) for s in SOURCES + HEADERS] + [os.path.join(ROOT, "include", "mdn.h")]
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and not _stale():
+        return LIB
+    os.makedirs(LIB_DIR, exist_ok=True)
+    cmd = [nvcc()] + NVCC_FLAGS + ["-shared", "-I", os.path.join(ROOT, "include"), "-I", CSRC]
+    cmd += [os.path.join(CSRC, s) for s in SOURCES] + ["-o", LIB + ".tmp"]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+def ptxas_report() -> str:
+    """Registers / spills / shared memory of the kernels (-Xptxas -v)."""
+    cmd = [nvcc()] + NVCC_FLAGS + ["-Xptxas", "-v", "-c", "-I", os.path.join(ROOT, "include"), "-I", CSRC,
+                                   os.path.join(CSRC, "advance.cu"), "-o", os.devnull]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    return r.stderr
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

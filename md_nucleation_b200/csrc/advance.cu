@@ -1,0 +1,1688 @@
+/*
+ * advance.cu -- the persistent step kernel of the engine (sm_100a).
+ *
+ * One launch advances a batch of replicas by n steps.  Thread-block clusters
+ * of C CTAs (C = the launch's cluster size, 1..8) pull replicas from a work
+ * queue, largest first, and keep a replica on-chip for all n steps:
+ *
+ *   - the "core" -- the ion (seed) and the in-domain vapor molecules, at most
+ *     a few hundred to ~1000 atoms -- lives in shared memory, replicated in
+ *     every CTA of the cluster.  All CTAs integrate it identically; its forces
+ *     are int64 fixed-point partial sums that the cluster adds over DSMEM, so
+ *     every copy receives the same total and the copies never diverge;
+ *   - the in-domain gas molecules (up to ~20,000 atoms) live in the gas slab in
+ *     global memory (L2-resident while the replica is being stepped) and are
+ *     split evenly over the cluster's CTAs;
+ *   - gas-gas interactions are absent from the reference's configurations, so
+ *     a gas molecule interacts only with the core: molecules whose gas-ion /
+ *     gas-vapor lists are empty ("far") are advanced by one thread in a single
+ *     pass (kick, drift, intramolecular force, kick); "near" molecules are
+ *     handled by one warp each, lanes striding over the list, with a
+ *     warp-shuffle reduction of the molecule's force and fixed-point atomics
+ *     for the reaction on the core.
+ *
+ * Each step follows MD::verlet (src/verlet.cpp:20-39) exactly:
+ *   kick (MD::velocity_calculation), [MD::velocity_scaling], drift with
+ *   optional SHAKE (MD::update_position / updatePositionSHAKE), ion centre and
+ *   taper weights, [MD::nosehoover_zeta], MD::check_pairlist -> make_pair on
+ *   the device, forces of every enabled Potential, kick, [MD::nosehoover_ion].
+ * The rebuild (MD::make_pair, src/pairList/pairlist.cpp:16-49) -- free flight,
+ * updateInCenters, in/out classification with periodic wrap and
+ * Maxwell-Boltzmann resampling, insertion with a random rotation, pair lists,
+ * loop_update -- runs inside the same launch, decided per replica.
+ *
+ * Precision: FP64 for integration, SHAKE, centres, weights, the rebuild and
+ * the bonded terms; FP32 for the pair terms (LJ, Coulomb, Born-Mayer-Huggins)
+ * on coordinates taken relative to the ion centre; every sum with more than one
+ * writer is an int64 fixed-point sum (units 2^-32 kcal/mol/A for forces,
+ * 2^-24 kcal/mol for energies), so results do not depend on the launch shape.
+ */
+#include <cooperative_groups.h>
+
+#include "device_util.cuh"
+#include "mdn_types.h"
+
+namespace cg = cooperative_groups;
+using namespace mdn;
+
+namespace {
+
+/* pointers into the dynamic shared memory of a CTA */
+struct Core {
+  double* x;        /* [3*nc] positions                        */
+  double* v;        /* [3*nc] velocities                       */
+  double* f;        /* [3*nc] force of the last evaluation     */
+  long long* acc;   /* [2][3*nc] fixed-point partial sums      */
+  double* xold;     /* [3*nc] positions before the drift       */
+  float4* pos;      /* [nc] (x - ion centre, charge), FP32     */
+  float* w;         /* [nc] taper weight                       */
+  int* type;        /* [nc] atom type                          */
+  int* mol;         /* [nc] -1 for ion atoms, else vapor slot  */
+  unsigned* excl;   /* AMBER exclusions, n_ion rows            */
+  float* ljA;       /* [nt*nt] 48 eps s^12                     */
+  float* ljB;       /* [nt*nt] 24 eps s^6                      */
+  double* c2;       /* [nt] 0.5*dt*4.184e-4 / mass             */
+  int* vcolor;      /* scratch                                 */
+};
+
+struct Ctx {
+  const KArgs* a;
+  RepParams* P;
+  RepDyn* D;
+  Core c;
+  int r;            /* replica                          */
+  int rank, C;      /* cluster rank and size            */
+  int n_core;       /* atoms in the core                */
+  int buf;          /* which acc buffer holds this step */
+  int* iscr;        /* >= 64 ints of scratch            */
+  double* dscr;     /* >= 64 doubles of scratch         */
+  const int* ib;    /* int blob of the replica          */
+  const double* db; /* double blob of the replica       */
+};
+
+__device__ __forceinline__ size_t gatom(const RepParams* P, int parity, int s, int a) {
+  return (size_t)P->slab_off + ((size_t)parity * P->slab_cap + s) * P->a_g + a;
+}
+__device__ __forceinline__ size_t gmol(const RepParams* P, int parity, int s) {
+  return (size_t)P->slab_moff + (size_t)parity * P->slab_cap + s;
+}
+__device__ __forceinline__ size_t vatom(const RepParams* P, int parity, int s, int a) {
+  return (size_t)P->vslab_off + ((size_t)parity * P->vcap + s) * P->a_v + a;
+}
+__device__ __forceinline__ size_t vmol(const RepParams* P, int parity, int s) {
+  return (size_t)P->vslab_moff + (size_t)parity * P->vcap + s;
+}
+
+__device__ __forceinline__ void set_status(const Ctx& x, int bit) {
+  atomicOr(&x.a->status[x.r], bit);
+}
+
+/* ------------------------------------------------------------------------- */
+/* core load / store                                                          */
+/* ------------------------------------------------------------------------- */
+__device__ void load_ion(Ctx& x) {
+  const RepParams* P = x.P;
+  const KArgs* a = x.a;
+  const int ni = P->n_ion;
+  for (int i = threadIdx.x; i < ni; i += blockDim.x) {
+    size_t g = (size_t)P->ion_off + i;
+    for (int k = 0; k < 3; k++) {
+      x.c.x[3 * i + k] = a->ion_x[3 * g + k];
+      x.c.v[3 * i + k] = a->ion_v[3 * g + k];
+      x.c.f[3 * i + k] = a->ion_f[3 * g + k];
+    }
+    x.c.type[i] = x.ib[P->o_ion_type + i];
+    x.c.mol[i] = -1;
+    x.c.w[i] = 1.0f;
+  }
+}
+
+/* the vapor part of the core, from the vapor slab of the current parity */
+__device__ void load_vapor(Ctx& x) {
+  const RepParams* P = x.P;
+  const KArgs* a = x.a;
+  const int ni = P->n_ion, av = P->a_v, nv = x.D->n_vap_in, par = x.D->parity;
+  x.n_core = ni + nv * av;
+  for (int t = threadIdx.x; t < nv * av; t += blockDim.x) {
+    int s = t / av, at = t - s * av;
+    size_t g = vatom(P, par, s, at);
+    int i = ni + t;
+    for (int k = 0; k < 3; k++) {
+      x.c.x[3 * i + k] = a->vslab_x[3 * g + k];
+      x.c.v[3 * i + k] = a->vslab_v[3 * g + k];
+      x.c.f[3 * i + k] = a->vslab_f[3 * g + k];
+    }
+    x.c.type[i] = x.ib[P->o_vap_type + at];
+    x.c.mol[i] = s;
+    x.c.w[i] = a->vslab_w[g];
+  }
+}
+
+__device__ void store_core(Ctx& x) {
+  const RepParams* P = x.P;
+  const KArgs* a = x.a;
+  if (x.rank != 0) return;
+  const int ni = P->n_ion, av = P->a_v, nv = x.D->n_vap_in, par = x.D->parity;
+  for (int i = threadIdx.x; i < ni; i += blockDim.x) {
+    size_t g = (size_t)P->ion_off + i;
+    for (int k = 0; k < 3; k++) {
+      a->ion_x[3 * g + k] = x.c.x[3 * i + k];
+      a->ion_v[3 * g + k] = x.c.v[3 * i + k];
+      a->ion_f[3 * g + k] = x.c.f[3 * i + k];
+    }
+  }
+  for (int t = threadIdx.x; t < nv * av; t += blockDim.x) {
+    int s = t / av, at = t - s * av;
+    size_t g = vatom(P, par, s, at);
+    int i = ni + t;
+    for (int k = 0; k < 3; k++) {
+      a->vslab_x[3 * g + k] = x.c.x[3 * i + k];
+      a->vslab_v[3 * g + k] = x.c.v[3 * i + k];
+      a->vslab_f[3 * g + k] = x.c.f[3 * i + k];
+    }
+    a->vslab_w[g] = x.c.w[i];
+  }
+}
+
+/* ------------------------------------------------------------------------- */
+/* integration of the core                                                    */
+/* ------------------------------------------------------------------------- */
+__device__ void core_kick(Ctx& x) {
+  for (int i = threadIdx.x; i < x.n_core; i += blockDim.x) {
+    double c2 = x.c.c2[x.c.type[i]];
+    for (int k = 0; k < 3; k++) x.c.v[3 * i + k] += x.c.f[3 * i + k] * c2;
+  }
+}
+
+/* Observer::computeProps, ion part: Tion.  Warp 0, lane-strided sums then a
+ * butterfly, so the result depends on the atom order only. */
+__device__ double ion_temperature(Ctx& x) {
+  const RepParams* P = x.P;
+  if (threadIdx.x < 32) {
+    double K = 0;
+    for (int i = threadIdx.x; i < P->n_ion; i += 32) {
+      double m = x.db[P->d_mass + x.c.type[i]];
+      K += x.c.v[3 * i] * x.c.v[3 * i] * m;
+      K += x.c.v[3 * i + 1] * x.c.v[3 * i + 1] * m;
+      K += x.c.v[3 * i + 2] * x.c.v[3 * i + 2] * m;
+    }
+    K = warp_sum_d(K);
+    if (threadIdx.x == 0) {
+      K *= 0.5 * P->real_to_kcalmol;
+      x.dscr[40] = K / double(P->n_ion) * ((1.0 / P->kb_real) / 1.5);
+    }
+  }
+  __syncthreads();
+  double T = x.dscr[40];
+  __syncthreads();
+  return T;
+}
+
+/* residual |s^2 - d^2| of constraint k */
+__device__ __forceinline__ double shake_residual(const double* X, int i, int j, double dk) {
+  double sx = X[3 * i] - X[3 * j], sy = X[3 * i + 1] - X[3 * j + 1], sz = X[3 * i + 2] - X[3 * j + 2];
+  double dr = sx * sx + sy * sy + sz * sz - dk * dk;
+  return dr * dr;
+}
+
+/* one SHAKE correction of constraint (i, j) with reference vector R_i - R_j */
+__device__ __forceinline__ void shake_pair(double* X, const double* R, int i, int j, double dk, double mi, double mj) {
+  double rx = R[3 * i] - R[3 * j], ry = R[3 * i + 1] - R[3 * j + 1], rz = R[3 * i + 2] - R[3 * j + 2];
+  double sx = X[3 * i] - X[3 * j], sy = X[3 * i + 1] - X[3 * j + 1], sz = X[3 * i + 2] - X[3 * j + 2];
+  double s2 = sx * sx + sy * sy + sz * sz;
+  double dot = rx * sx + ry * sy + rz * sz;
+  double minv = 1 / mi + 1 / mj;
+  if (dot < 1e-10) dot = 1e-10;
+  double g = (dk * dk - s2) / (2 * minv * dot);
+  double ci = g / mi, cj = g / mj;
+  X[3 * i] += rx * ci; X[3 * i + 1] += ry * ci; X[3 * i + 2] += rz * ci;
+  X[3 * j] -= rx * cj; X[3 * j + 1] -= ry * cj; X[3 * j + 2] -= rz * cj;
+}
+
+/* SHAKE of one small molecule by one thread (vapor, gas): sweeps in colour
+ * order until every constraint satisfies (s^2 - d^2)^2 <= 1e-20 after a sweep */
+__device__ int shake_small(const Ctx& x, double* X, double* V, const double* R, const double* m, int n,
+                           const int* rigid, int n_rigid, const int* color, int n_colors, bool vcorr) {
+  const RepParams* P = x.P;
+  double X0[3 * MDN_MAX_VAP_ATOMS];
+  for (int q = 0; q < 3 * n; q++) X0[q] = X[q];
+  bool converge = false;
+  for (int sweep = 0; sweep < MDN_SHAKE_MAX_SWEEPS && !converge; sweep++) {
+    for (int c = 0; c < n_colors; c++)
+      for (int k = 0; k < n_rigid; k++) {
+        if (color[k] != c) continue;
+        int i = rigid[3 * k], j = rigid[3 * k + 1];
+        shake_pair(X, R, i, j, x.db[P->d_bond + 2 * rigid[3 * k + 2] + 1], m[i], m[j]);
+      }
+    converge = true;
+    for (int k = 0; k < n_rigid; k++)
+      if (shake_residual(X, rigid[3 * k], rigid[3 * k + 1], x.db[P->d_bond + 2 * rigid[3 * k + 2] + 1]) > 1e-20)
+        converge = false;
+  }
+  if (vcorr)
+    for (int q = 0; q < 3 * n; q++) V[q] += (X[q] - X0[q]) / P->dt;
+  return converge ? 0 : MDN_ST_SHAKE_NOCONV;
+}
+
+__device__ void core_drift_shake(Ctx& x) {
+  const RepParams* P = x.P;
+  const bool sh = (P->interactions & MDN_I_SHAKE) != 0;
+  const bool vcorr = !(P->quirks & MDN_Q_SHAKE_NO_VCORR);
+  const double dt = P->dt;
+  for (int i = threadIdx.x; i < x.n_core; i += blockDim.x) {
+    for (int k = 0; k < 3; k++) {
+      double xo = x.c.x[3 * i + k];
+      x.c.xold[3 * i + k] = xo;
+      x.c.x[3 * i + k] = xo + x.c.v[3 * i + k] * dt;
+    }
+  }
+  __syncthreads();
+  if (!sh) return;
+  /* ion: block-parallel sweeps, one colour at a time; a colour's constraints
+   * share no atom, so the sweep equals the sequential colour-ordered sweep */
+  if (P->n_ion_rigid > 0) {
+    const int* rig = x.ib + P->o_ion_rigid;
+    const int* col = x.ib + P->o_ion_color;
+    int sweeps = 0;
+    for (;;) {
+      for (int c = 0; c < P->n_ion_colors; c++) {
+        for (int k = threadIdx.x; k < P->n_ion_rigid; k += blockDim.x) {
+          if (col[k] != c) continue;
+          int i = rig[3 * k], j = rig[3 * k + 1];
+          shake_pair(x.c.x, x.c.xold, i, j, x.db[P->d_bond + 2 * rig[3 * k + 2] + 1],
+                     x.db[P->d_mass + x.c.type[i]], x.db[P->d_mass + x.c.type[j]]);
+        }
+        __syncthreads();
+      }
+      if (threadIdx.x == 0) x.iscr[50] = 1;
+      __syncthreads();
+      for (int k = threadIdx.x; k < P->n_ion_rigid; k += blockDim.x)
+        if (shake_residual(x.c.x, rig[3 * k], rig[3 * k + 1], x.db[P->d_bond + 2 * rig[3 * k + 2] + 1]) > 1e-20)
+          x.iscr[50] = 0;
+      __syncthreads();
+      int conv = x.iscr[50];
+      __syncthreads();
+      if (conv) break;
+      if (++sweeps >= MDN_SHAKE_MAX_SWEEPS) {
+        if (threadIdx.x == 0 && x.rank == 0) set_status(x, MDN_ST_SHAKE_NOCONV);
+        break;
+      }
+    }
+    if (vcorr)
+      for (int i = threadIdx.x; i < P->n_ion; i += blockDim.x)
+        for (int k = 0; k < 3; k++) {
+          /* displacement by the constraints = x - (xold + v*dt) */
+          double xd = x.c.xold[3 * i + k] + x.c.v[3 * i + k] * dt;
+          x.c.v[3 * i + k] += (x.c.x[3 * i + k] - xd) / dt;
+        }
+    __syncthreads();
+  }
+  /* vapor molecules: one thread each */
+  if (P->n_vap_rigid > 0) {
+    const int av = P->a_v;
+    for (int s = threadIdx.x; s < x.D->n_vap_in; s += blockDim.x) {
+      int base = P->n_ion + s * av;
+      double X[3 * MDN_MAX_VAP_ATOMS], V[3 * MDN_MAX_VAP_ATOMS], R[3 * MDN_MAX_VAP_ATOMS], m[MDN_MAX_VAP_ATOMS];
+      double Xd[3 * MDN_MAX_VAP_ATOMS];
+      for (int at = 0; at < av; at++) {
+        m[at] = x.db[P->d_mass + x.c.type[base + at]];
+        for (int k = 0; k < 3; k++) {
+          X[3 * at + k] = x.c.x[3 * (base + at) + k];
+          V[3 * at + k] = x.c.v[3 * (base + at) + k];
+          R[3 * at + k] = x.c.xold[3 * (base + at) + k];
+          Xd[3 * at + k] = X[3 * at + k];
+        }
+      }
+      int st = shake_small(x, X, V, R, m, av, x.ib + P->o_vap_rigid, P->n_vap_rigid, x.ib + P->o_vap_color,
+                           P->n_vap_colors, false);
+      if (st && x.rank == 0) set_status(x, st);
+      for (int at = 0; at < av; at++)
+        for (int k = 0; k < 3; k++) {
+          x.c.x[3 * (base + at) + k] = X[3 * at + k];
+          if (vcorr) x.c.v[3 * (base + at) + k] += (X[3 * at + k] - Xd[3 * at + k]) / P->dt;
+        }
+    }
+  }
+  __syncthreads();
+}
+
+/* ion centre: warp 0, lane-strided partial sums, butterfly, fixed order */
+__device__ void ion_centre(Ctx& x) {
+  const RepParams* P = x.P;
+  if (threadIdx.x < 32) {
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = threadIdx.x; i < P->n_ion; i += 32) {
+      double m = x.db[P->d_mass + x.c.type[i]];
+      for (int k = 0; k < 3; k++) {
+        s[k] += x.c.x[3 * i + k] * m;
+        s[3 + k] += x.c.v[3 * i + k] * m;
+      }
+    }
+    for (int k = 0; k < 6; k++) s[k] = warp_sum_d(s[k]);
+    if (threadIdx.x == 0) {
+      double mInv = 1 / P->ion_msum;
+      for (int k = 0; k < 6; k++) x.D->ion_com[k] = s[k] * mInv;
+    }
+  }
+  __syncthreads();
+}
+
+/* the ion centre in the reference's own order (sequential sum), used where a
+ * threshold decision depends on it (the in/out classification) */
+__device__ void ion_centre_exact(Ctx& x) {
+  const RepParams* P = x.P;
+  if (threadIdx.x == 0) {
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = 0; i < P->n_ion; i++) {
+      double m = x.db[P->d_mass + x.c.type[i]];
+      for (int k = 0; k < 3; k++) {
+        s[k] += x.c.x[3 * i + k] * m;
+        s[3 + k] += x.c.v[3 * i + k] * m;
+      }
+    }
+    double mInv = 1 / P->ion_msum;
+    for (int k = 0; k < 6; k++) x.D->ion_com[k] = s[k] * mInv;
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ double taper(const RepParams* P, const double* com, const double* xa) {
+  double dx = xa[0] - com[0];
+  double dy = xa[1] - com[1];
+  double dz = xa[2] - com[2];
+  double r2 = dx * dx + dy * dy + dz * dz;
+  if (r2 < P->ri2) return 1;
+  if (r2 > P->RI2) return 0;
+  double dr = (sqrt(r2) - P->rcenter);
+  double C = cos(3.141592653589793 / P->overlap * 0.5 * dr);
+  return C * C;
+}
+
+/* taper weights of the vapor atoms (when `weights`) and the FP32 coordinates
+ * of the core relative to the ion centre.  A molecule inserted by the rebuild
+ * of this step carries w < 0 and gets 0 for this step: MD::update_position
+ * ran before the rebuild, while the molecule was still outside
+ * (src/verlet.cpp:109-134), so the reference leaves its weights unset. */
+__device__ void core_weights_pos(Ctx& x, bool weights) {
+  const RepParams* P = x.P;
+  const double* com = x.D->ion_com;
+  for (int i = threadIdx.x; i < x.n_core; i += blockDim.x) {
+    if (i >= P->n_ion) {
+      if (x.c.w[i] < 0.0f) x.c.w[i] = 0.0f;
+      else if (weights) x.c.w[i] = (float)taper(P, com, x.c.x + 3 * i);
+    }
+    double q = i < P->n_ion ? x.db[P->d_ion_q + i] : x.db[P->d_vap_q + (i - P->n_ion) % P->a_v];
+    x.c.pos[i] = make_float4((float)(x.c.x[3 * i] - com[0]), (float)(x.c.x[3 * i + 1] - com[1]),
+                             (float)(x.c.x[3 * i + 2] - com[2]), (float)q);
+  }
+  __syncthreads();
+}
+
+/* ------------------------------------------------------------------------- */
+/* bonded terms (FP64, the reference's expressions)                           */
+/* ------------------------------------------------------------------------- */
+struct BondOut {
+  double f[4][3];
+  double e;
+};
+
+__device__ __forceinline__ void bond_fd(const double* X, const double* co, int i, int j, BondOut& o) {
+  double dx = X[3 * i] - X[3 * j];
+  double dy = X[3 * i + 1] - X[3 * j + 1];
+  double dz = X[3 * i + 2] - X[3 * j + 2];
+  double rsq = (dx * dx + dy * dy + dz * dz);
+  double r = sqrt(rsq);
+  double dr = (r - co[1]);
+  double rk = co[0] * dr;
+  double fb = -2.0 * rk / r;
+  o.f[0][0] = fb * dx; o.f[0][1] = fb * dy; o.f[0][2] = fb * dz;
+  o.f[1][0] = -(fb * dx); o.f[1][1] = -(fb * dy); o.f[1][2] = -(fb * dz);
+  o.e = rk * dr;
+}
+
+__device__ __forceinline__ void angle_fd(const double* X, const double* co, int i, int j, int k, BondOut& o) {
+  double dx1 = X[3 * i] - X[3 * j];
+  double dy1 = X[3 * i + 1] - X[3 * j + 1];
+  double dz1 = X[3 * i + 2] - X[3 * j + 2];
+  double rsq1 = (dx1 * dx1 + dy1 * dy1 + dz1 * dz1);
+  double r1 = sqrt(rsq1);
+  double dx2 = X[3 * k] - X[3 * j];
+  double dy2 = X[3 * k + 1] - X[3 * j + 1];
+  double dz2 = X[3 * k + 2] - X[3 * j + 2];
+  double rsq2 = (dx2 * dx2 + dy2 * dy2 + dz2 * dz2);
+  double r2 = sqrt(rsq2);
+  double C = dx1 * dx2 + dy1 * dy2 + dz1 * dz2;
+  C /= r1 * r2;
+  double Cs = 1 / (sqrt(1.0 - C * C));
+  double dtheta = acos(C) - co[1];
+  double tk = co[0] * dtheta;
+  double a = -2.0 * tk * Cs;
+  double a11 = a * C / rsq1;
+  double a12 = -a / (r1 * r2);
+  double a22 = a * C / rsq2;
+  double f1[3] = {a11 * dx1 + a12 * dx2, a11 * dy1 + a12 * dy2, a11 * dz1 + a12 * dz2};
+  double f3[3] = {a22 * dx2 + a12 * dx1, a22 * dy2 + a12 * dy1, a22 * dz2 + a12 * dz1};
+  for (int q = 0; q < 3; q++) {
+    o.f[0][q] = f1[q];
+    o.f[1][q] = -(f1[q] + f3[q]);
+    o.f[2][q] = f3[q];
+  }
+  o.e = tk * dtheta;
+}
+
+__device__ __forceinline__ void dihedral_fd(const double* X, const double* co, int multi, int i, int j, int k,
+                                            int l, BondOut& o) {
+  double vb1x = X[3 * i] - X[3 * j];
+  double vb1y = X[3 * i + 1] - X[3 * j + 1];
+  double vb1z = X[3 * i + 2] - X[3 * j + 2];
+  double vb2x = X[3 * k] - X[3 * j];
+  double vb2y = X[3 * k + 1] - X[3 * j + 1];
+  double vb2z = X[3 * k + 2] - X[3 * j + 2];
+  double vb2xm = -vb2x, vb2ym = -vb2y, vb2zm = -vb2z;
+  double vb3x = X[3 * l] - X[3 * k];
+  double vb3y = X[3 * l + 1] - X[3 * k + 1];
+  double vb3z = X[3 * l + 2] - X[3 * k + 2];
+  double ax = vb1y * vb2zm - vb1z * vb2ym;
+  double ay = vb1z * vb2xm - vb1x * vb2zm;
+  double az = vb1x * vb2ym - vb1y * vb2xm;
+  double bx = vb3y * vb2zm - vb3z * vb2ym;
+  double by = vb3z * vb2xm - vb3x * vb2zm;
+  double bz = vb3x * vb2ym - vb3y * vb2xm;
+  double rasq = ax * ax + ay * ay + az * az;
+  double rbsq = bx * bx + by * by + bz * bz;
+  double rgsq = vb2xm * vb2xm + vb2ym * vb2ym + vb2zm * vb2zm;
+  double rg = sqrt(rgsq);
+  double rginv = 0.0, ra2inv = 0.0, rb2inv = 0.0;
+  if (rg > 0) rginv = 1.0 / rg;
+  if (rasq > 0) ra2inv = 1.0 / rasq;
+  if (rbsq > 0) rb2inv = 1.0 / rbsq;
+  double rabinv = sqrt(ra2inv * rb2inv);
+  double c = (ax * bx + ay * by + az * bz) * rabinv;
+  double s = rg * rabinv * (ax * vb3x + ay * vb3y + az * vb3z);
+  double df = 0.0, e = 0.0;
+  for (int JJ = 0; JJ < multi; JJ++) {
+    int J5 = JJ * 5;
+    double p_ = 1.0, df1 = 0.0, ddf1 = 0.0;
+    for (int loop = 0; loop < co[J5 + 1]; loop++) {
+      ddf1 = p_ * c - df1 * s;
+      df1 = p_ * s + df1 * c;
+      p_ = ddf1;
+    }
+    p_ = p_ * co[J5 + 3] + df1 * co[J5 + 4];
+    df1 = df1 * co[J5 + 3] - ddf1 * co[J5 + 4];
+    df1 *= -co[J5 + 1];
+    p_ += 1.0;
+    if (co[1] == 0) { /* term 0's periodicity tested for every term (src/potential/compute_AMBER.cpp:199) */
+      p_ = 1.0 + co[J5 + 3];
+      df1 = 0.0;
+    }
+    df += (-co[J5] * df1);
+    e += co[J5] * p_;
+  }
+  double fg = vb1x * vb2xm + vb1y * vb2ym + vb1z * vb2zm;
+  double hg = vb3x * vb2xm + vb3y * vb2ym + vb3z * vb2zm;
+  double fga = fg * ra2inv * rginv;
+  double hgb = hg * rb2inv * rginv;
+  double gaa = -ra2inv * rg;
+  double gbb = rb2inv * rg;
+  double dtf[3] = {gaa * ax, gaa * ay, gaa * az};
+  double dtg[3] = {fga * ax - hgb * bx, fga * ay - hgb * by, fga * az - hgb * bz};
+  double dth[3] = {gbb * bx, gbb * by, gbb * bz};
+  for (int q = 0; q < 3; q++) {
+    double s2 = df * dtg[q];
+    double f1 = df * dtf[q];
+    double f4 = df * dth[q];
+    o.f[0][q] = f1;
+    o.f[1][q] = s2 - f1;
+    o.f[2][q] = -s2 - f4;
+    o.f[3][q] = f4;
+  }
+  o.e = e;
+}
+
+/* ------------------------------------------------------------------------- */
+/* FP32 pair terms                                                            */
+/* ------------------------------------------------------------------------- */
+/* LJ (+ Coulomb) force factor and energy, the reference's formulas:
+ *   f = r^-6 (A r^-6 - B) r^-2 [+ qqrd2e qi qj r^-1 r^-2], times w
+ *   U = r^-6 (A/12 r^-6 - B/6) [+ qqrd2e qi qj / r]  (unweighted)          */
+__device__ __forceinline__ float lj_coul(float r2, float A, float B, float qq, bool coul, float* e) {
+  float rinv = rsqrtf(r2);
+  float r2inv = rinv * rinv;
+  float r6inv = r2inv * r2inv * r2inv;
+  float flj = r6inv * fmaf(A, r6inv, -B);
+  float fc = coul ? qq * rinv : 0.0f;
+  *e = fmaf(r6inv, fmaf(A * (1.0f / 12.0f), r6inv, -B * (1.0f / 6.0f)), fc);
+  return (flj + fc) * r2inv;
+}
+
+/* pair energies in FP64 from FP64 coordinates, evaluated only on the steps
+ * that request energies: sums of Coulomb terms of both signs cancel by orders
+ * of magnitude, which FP32 coordinates cannot resolve */
+__device__ __forceinline__ double r2d(const double* a, const double* b) {
+  double dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
+  return dx * dx + dy * dy + dz * dz;
+}
+__device__ __forceinline__ double lj_coul_energy(double r2, double A, double B, double qq) {
+  double r2inv = 1 / r2;
+  double r6inv = r2inv * r2inv * r2inv;
+  return r6inv * (A / 12.0 * r6inv - B / 6.0) + qq * sqrt(r2inv);
+}
+
+/* Born-Mayer-Huggins (Tosi-Fumi NaCl, src/potential/BMHFT/potentialBMHFT.hpp:21-39) */
+__constant__ float kBorn[2][2][5] = {
+    {{25.4435f * 3.1546f / 4.184f, 6.f * 101.1719f / 4.184f, 8.f * 48.1771f / 4.184f, 2.340f, 3.1546f},
+     {20.3548f * 3.1546f / 4.184f, 6.f * 674.4793f / 4.184f, 8.f * 837.077f / 4.184f, 2.755f, 3.1546f}},
+    {{20.3548f * 3.1546f / 4.184f, 6.f * 674.4793f / 4.184f, 8.f * 837.077f / 4.184f, 2.755f, 3.1546f},
+     {15.2661f * 3.1546f / 4.184f, 6.f * 6985.6786f / 4.184f, 8.f * 14031.5785f / 4.184f, 3.170f, 3.1546f}}};
+
+__device__ __forceinline__ double born_energy(double r2, int ti, int tj, double qq) {
+  const float* c = kBorn[ti][tj];
+  double r2inv = 1 / r2;
+  double r6inv = r2inv * r2inv * r2inv;
+  double r = sqrt(r2);
+  double rexp = exp((double)c[4] * ((double)c[3] - r));
+  return qq * sqrt(r2inv) + rexp * c[0] - (double)c[1] / 6.0 * r6inv - (double)c[2] / 8.0 * r6inv * r2inv;
+}
+
+__device__ __forceinline__ float born(float r2, int ti, int tj, float qq, float* e) {
+  const float* c = kBorn[ti][tj];
+  float rinv = rsqrtf(r2);
+  float r = r2 * rinv;
+  float r2inv = rinv * rinv;
+  float r6inv = r2inv * r2inv * r2inv;
+  float rexp = expf(c[4] * (c[3] - r));
+  float f1 = c[4] * c[0] * r * rexp;
+  float f2 = -c[1] * r6inv;
+  float f3 = -c[2] * r6inv * r2inv;
+  float fc = qq * rinv;
+  *e = fc + rexp * c[0] - c[1] * (1.0f / 6.0f) * r6inv - c[2] * (1.0f / 8.0f) * r6inv * r2inv;
+  return (f1 + f2 + f3 + fc) * r2inv;
+}
+
+/* ------------------------------------------------------------------------- */
+/* forces of the core (ion + vapor) among themselves, and the core kick        */
+/* ------------------------------------------------------------------------- */
+__device__ __forceinline__ void acc_add(Ctx& x, int i, const long long* f3) {
+  long long* A = x.c.acc + (size_t)x.buf * 3 * x.a->nc_cap + 3 * i;
+  atomicAdd((unsigned long long*)&A[0], (unsigned long long)f3[0]);
+  atomicAdd((unsigned long long*)&A[1], (unsigned long long)f3[1]);
+  atomicAdd((unsigned long long*)&A[2], (unsigned long long)f3[2]);
+}
+
+__device__ __forceinline__ void energy_add(Ctx& x, int bucket, long long e) {
+  if (e != 0) atomicAdd((unsigned long long*)&x.a->energy[8 * x.r + bucket], (unsigned long long)e);
+}
+
+__device__ __forceinline__ bool term_on(const Ctx& x, unsigned bit) {
+  return (x.P->interactions & bit) && (!x.a->term_mask || (x.a->term_mask & bit));
+}
+
+__device__ void core_pairs(Ctx& x, bool eflag) {
+  const RepParams* P = x.P;
+  const int ni = P->n_ion, nc = x.n_core, nt = P->n_types;
+  const bool amber = term_on(x, MDN_I_AMBER), bmh = term_on(x, MDN_I_BMH);
+  const bool vi = term_on(x, MDN_I_VI), vv = term_on(x, MDN_I_VV);
+  if (!(amber || bmh || vi || vv)) return;
+  const float qqf = (float)P->qqrd2e;
+  const int nblk = (nc + 31) >> 5;
+  const long long items = (long long)nc * nblk;
+  const int* bmht = x.ib + P->o_ion_bmh;
+  long long eU[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (long long it = (long long)x.rank * blockDim.x + threadIdx.x; it < items;
+       it += (long long)x.C * blockDim.x) {
+    int i = (int)(it / nblk), jb = (int)(it - (long long)i * nblk);
+    float4 pi = x.c.pos[i];
+    int ti = x.c.type[i];
+    int mi = x.c.mol[i];
+    float wi = x.c.w[i];
+    bool iion = i < ni;
+    long long F[3] = {0, 0, 0};
+    int j1 = min(nc, (jb + 1) * 32);
+    for (int j = jb * 32; j < j1; j++) {
+      if (j == i) continue;
+      bool jion = j < ni;
+      float4 pj = x.c.pos[j];
+      float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+      float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      float fp = 0.0f, e = 0.0f;
+      int bucket = 0;
+      bool any = false;
+      if (iion && jion) {
+        if (amber && !((x.c.excl[i * P->excl_words + (j >> 5)] >> (j & 31)) & 1u)) {
+          int tj = x.c.type[j];
+          float ee;
+          fp += lj_coul(r2, x.c.ljA[ti * nt + tj], x.c.ljB[ti * nt + tj], qqf * pi.w * pj.w, true, &ee);
+          e += ee;
+          any = true;
+        }
+        if (bmh) {
+          float ee;
+          fp += born(r2, bmht[i], bmht[j], qqf * pi.w * pj.w, &ee);
+          e += ee;
+          any = true;
+        }
+        bucket = MDN_U_ION;
+      } else if (iion != jion) {
+        if (vi) {
+          int tj = x.c.type[j];
+          float ee;
+          fp = lj_coul(r2, x.c.ljA[ti * nt + tj], x.c.ljB[ti * nt + tj], qqf * pi.w * pj.w, true, &ee) *
+               (wi * x.c.w[j]);
+          e = ee;
+          any = true;
+          bucket = MDN_U_VI;
+        }
+      } else if (mi != x.c.mol[j]) {
+        if (vv) {
+          int tj = x.c.type[j];
+          float ee;
+          fp = lj_coul(r2, x.c.ljA[ti * nt + tj], x.c.ljB[ti * nt + tj], qqf * pi.w * pj.w, true, &ee) *
+               (wi * x.c.w[j]);
+          e = ee;
+          any = true;
+          bucket = MDN_U_VV;
+        }
+      }
+      if (!any) continue;
+      F[0] += fixf(fp * dx);
+      F[1] += fixf(fp * dy);
+      F[2] += fixf(fp * dz);
+      if (eflag && j > i) {
+        const double R2 = r2d(x.c.x + 3 * i, x.c.x + 3 * j);
+        const double qi = i < ni ? x.db[P->d_ion_q + i] : x.db[P->d_vap_q + (i - ni) % P->a_v];
+        const double qj = j < ni ? x.db[P->d_ion_q + j] : x.db[P->d_vap_q + (j - ni) % P->a_v];
+        const double qq = P->qqrd2e * qi * qj;
+        const int tj = x.c.type[j];
+        double ed = 0;
+        if (bucket == MDN_U_ION) {
+          if (amber && !((x.c.excl[i * P->excl_words + (j >> 5)] >> (j & 31)) & 1u))
+            ed += lj_coul_energy(R2, x.db[P->d_ljA + ti * nt + tj], x.db[P->d_ljB + ti * nt + tj], qq);
+          if (bmh) ed += born_energy(R2, bmht[i], bmht[j], qq);
+        } else {
+          ed = lj_coul_energy(R2, x.db[P->d_ljA + ti * nt + tj], x.db[P->d_ljB + ti * nt + tj], qq);
+        }
+        eU[bucket] += efixd(ed);
+      }
+      (void)e;
+    }
+    if (F[0] | F[1] | F[2]) acc_add(x, i, F);
+  }
+  if (eflag)
+    for (int b = 0; b < 8; b++) {
+      long long s = warp_sum_ll(eU[b]);
+      if ((threadIdx.x & 31) == 0) energy_add(x, b, s);
+    }
+}
+
+__device__ void core_bonded(Ctx& x, bool eflag) {
+  const RepParams* P = x.P;
+  const bool amber = term_on(x, MDN_I_AMBER);
+  const bool vin = term_on(x, MDN_I_VAPOR_INTRA);
+  const bool qb = (P->quirks & MDN_Q_ENERGY_BUCKETS) != 0;
+  const int nb = amber ? P->n_ion_bonds : 0, na = amber ? P->n_ion_angles : 0, nd = amber ? P->n_ion_dih : 0;
+  const int vterms = vin ? (P->n_vap_bonds + P->n_vap_angles + P->n_vap_dih) : 0;
+  const long long total = (long long)nb + na + nd + (long long)vterms * x.D->n_vap_in;
+  long long eU[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (long long t = (long long)x.rank * blockDim.x + threadIdx.x; t < total; t += (long long)x.C * blockDim.x) {
+    BondOut o;
+    int idx[4];
+    int n = 0, bucket = MDN_U_ION;
+    const double* X = x.c.x;
+    int base = 0;
+    long long u = t;
+    int kind;  /* 0 bond, 1 angle, 2 dihedral */
+    const int* row;
+    if (u < nb) { kind = 0; row = x.ib + P->o_ion_bonds + 3 * u; }
+    else if ((u -= nb) < na) { kind = 1; row = x.ib + P->o_ion_angles + 4 * u; }
+    else if ((u -= na) < nd) { kind = 2; row = x.ib + P->o_ion_dih + 5 * u; }
+    else {
+      u -= nd;
+      int s = (int)(u / vterms), q = (int)(u - (long long)s * vterms);
+      base = P->n_ion + s * P->a_v;
+      if (q < P->n_vap_bonds) { kind = 0; row = x.ib + P->o_vap_bonds + 3 * q; bucket = qb ? MDN_U_GAS : MDN_U_VAP; }
+      else if ((q -= P->n_vap_bonds) < P->n_vap_angles) { kind = 1; row = x.ib + P->o_vap_angles + 4 * q; bucket = qb ? MDN_U_GAS : MDN_U_VAP; }
+      else { q -= P->n_vap_angles; kind = 2; row = x.ib + P->o_vap_dih + 5 * q; bucket = qb ? MDN_U_ION : MDN_U_VAP; }
+    }
+    if (kind == 0) {
+      idx[0] = base + row[0]; idx[1] = base + row[1];
+      bond_fd(X, x.db + P->d_bond + 2 * row[2], idx[0], idx[1], o);
+      n = 2;
+    } else if (kind == 1) {
+      idx[0] = base + row[0]; idx[1] = base + row[1]; idx[2] = base + row[2];
+      angle_fd(X, x.db + P->d_angle + 2 * row[3], idx[0], idx[1], idx[2], o);
+      n = 3;
+    } else {
+      idx[0] = base + row[0]; idx[1] = base + row[1]; idx[2] = base + row[2]; idx[3] = base + row[3];
+      dihedral_fd(X, x.db + P->d_dih + 15 * row[4], x.ib[P->o_dih_multi + row[4]], idx[0], idx[1], idx[2],
+                  idx[3], o);
+      n = 4;
+    }
+    for (int q = 0; q < n; q++) {
+      long long F[3] = {fixd(o.f[q][0]), fixd(o.f[q][1]), fixd(o.f[q][2])};
+      acc_add(x, idx[q], F);
+    }
+    if (eflag) eU[bucket] += efixd(o.e);
+  }
+  if (eflag)
+    for (int b = 0; b < 8; b++) {
+      long long s = warp_sum_ll(eU[b]);
+      if ((threadIdx.x & 31) == 0) energy_add(x, b, s);
+    }
+  if (term_on(x, MDN_I_EFIELD) && x.rank == 0)
+    for (int i = threadIdx.x; i < P->n_ion; i += blockDim.x) {
+      double coeff = 5.55e-5 * x.db[P->d_ion_q + i];
+      long long F[3] = {fixd(coeff * P->efield[0]), fixd(coeff * P->efield[1]), fixd(coeff * P->efield[2])};
+      acc_add(x, i, F);
+    }
+}
+
+/* ------------------------------------------------------------------------- */
+/* gas molecules                                                              */
+/* ------------------------------------------------------------------------- */
+__device__ __forceinline__ void partition(const Ctx& x, int n, int* lo, int* hi) {
+  *lo = (int)(((long long)n * x.rank) / x.C);
+  *hi = (int)(((long long)n * (x.rank + 1)) / x.C);
+}
+
+/* intramolecular bond force of one gas molecule (PotentialGasIntra), FP64 */
+__device__ __forceinline__ double gas_intra(const Ctx& x, const double* X, double* F) {
+  const RepParams* P = x.P;
+  double e = 0;
+  for (int b = 0; b < P->n_gas_bonds; b++) {
+    const int* row = x.ib + P->o_gas_bonds + 3 * b;
+    BondOut o;
+    bond_fd(X, x.db + P->d_bond + 2 * row[2], row[0], row[1], o);
+    for (int k = 0; k < 3; k++) {
+      F[3 * row[0] + k] += o.f[0][k];
+      F[3 * row[1] + k] += o.f[1][k];
+    }
+    e += o.e;
+  }
+  return e;
+}
+
+/* kick + drift (+SHAKE) of the gas molecules of this CTA; far molecules also
+ * get their intramolecular force and the second kick when `fused`. */
+__device__ void gas_integrate(Ctx& x, bool fused, bool eflag) {
+  const RepParams* P = x.P;
+  const KArgs* a = x.a;
+  const int ag = P->a_g, par = x.D->parity;
+  const bool sh = (P->interactions & MDN_I_SHAKE) && P->n_gas_rigid > 0;
+  const bool vcorr = !(P->quirks & MDN_Q_SHAKE_NO_VCORR);
+  const bool intra = term_on(x, MDN_I_GAS_INTRA) && P->n_gas_bonds > 0;
+  const double dt = P->dt;
+  int lo, hi;
+  partition(x, x.D->n_gas_in, &lo, &hi);
+  double m[MDN_MAX_GAS_ATOMS], c2[MDN_MAX_GAS_ATOMS];
+  for (int at = 0; at < ag; at++) {
+    int t = x.ib[P->o_gas_type + at];
+    m[at] = x.db[P->d_mass + t];
+    c2[at] = x.c.c2[t];
+  }
+  long long eg = 0;
+  for (int s = lo + threadIdx.x; s < hi; s += blockDim.x) {
+    double X[3 * MDN_MAX_GAS_ATOMS], V[3 * MDN_MAX_GAS_ATOMS], F[3 * MDN_MAX_GAS_ATOMS], R[3 * MDN_MAX_GAS_ATOMS];
+    for (int at = 0; at < ag; at++) {
+      size_t g = gatom(P, par, s, at);
+      for (int k = 0; k < 3; k++) {
+        X[3 * at + k] = a->slab_x[3 * g + k];
+        V[3 * at + k] = a->slab_v[3 * g + k];
+        F[3 * at + k] = a->slab_f[3 * g + k];
+      }
+    }
+    for (int at = 0; at < ag; at++)
+      for (int k = 0; k < 3; k++) {
+        V[3 * at + k] += F[3 * at + k] * c2[at];
+        R[3 * at + k] = X[3 * at + k];
+        X[3 * at + k] = X[3 * at + k] + V[3 * at + k] * dt;
+        F[3 * at + k] = 0.0;
+      }
+    if (sh) {
+      double Xd[3 * MDN_MAX_GAS_ATOMS];
+      for (int q = 0; q < 3 * ag; q++) Xd[q] = X[q];
+      int zero = 0;
+      int st = shake_small(x, X, V, R, m, ag, x.ib + P->o_gas_rigid, P->n_gas_rigid, &zero, 1, false);
+      if (st) set_status(x, st);
+      if (vcorr)
+        for (int q = 0; q < 3 * ag; q++) V[q] += (X[q] - Xd[q]) / dt;
+    }
+    bool near = fused ? (a->near_gi[gmol(P, par, s)] >= 0) : true;
+    if (!near) {
+      if (intra) {
+        double e = gas_intra(x, X, F);
+        if (eflag) eg += efixd(e);
+      }
+      for (int at = 0; at < ag; at++)
+        for (int k = 0; k < 3; k++) V[3 * at + k] += F[3 * at + k] * c2[at];
+    }
+    for (int at = 0; at < ag; at++) {
+      size_t g = gatom(P, par, s, at);
+      for (int k = 0; k < 3; k++) {
+        a->slab_x[3 * g + k] = X[3 * at + k];
+        a->slab_v[3 * g + k] = V[3 * at + k];
+        a->slab_f[3 * g + k] = F[3 * at + k];
+      }
+    }
+  }
+  if (eflag && intra) {
+    eg = warp_sum_ll(eg);
+    if ((threadIdx.x & 31) == 0) energy_add(x, MDN_U_GAS, eg);
+  }
+}
+
+/* after a rebuild: intramolecular force and second kick of the far molecules */
+__device__ void gas_far_pass(Ctx& x, bool eflag, bool kick) {
+  const RepParams* P = x.P;
+  const KArgs* a = x.a;
+  const int ag = P->a_g, par = x.D->parity;
+  const bool intra = term_on(x, MDN_I_GAS_INTRA) && P->n_gas_bonds > 0;
+  int lo, hi;
+  partition(x, x.D->n_gas_in, &lo, &hi);
+  double c2[MDN_MAX_GAS_ATOMS];
+  for (int at = 0; at < ag; at++) c2[at] = x.c.c2[x.ib[P->o_gas_type + at]];
+  long long eg = 0;
+  for (int s = lo + threadIdx.x; s < hi; s += blockDim.x) {
+    if (a->near_gi[gmol(P, par, s)] >= 0) continue;
+    double X[3 * MDN_MAX_GAS_ATOMS], F[3 * MDN_MAX_GAS_ATOMS];
+    for (int at = 0; at < ag; at++) {
+      size_t g = gatom(P, par, s, at);
+      for (int k = 0; k < 3; k++) {
+        X[3 * at + k] = a->slab_x[3 * g + k];
+        F[3 * at + k] = 0.0;
+      }
+    }
+    if (intra) {
+      double e = gas_intra(x, X, F);
+      if (eflag) eg += efixd(e);
+    }
+    for (int at = 0; at < ag; at++) {
+      size_t g = gatom(P, par, s, at);
+      for (int k = 0; k < 3; k++) {
+        if (kick) a->slab_v[3 * g + k] += F[3 * at + k] * c2[at];
+        a->slab_f[3 * g + k] = F[3 * at + k];
+      }
+    }
+  }
+  if (eflag && intra) {
+    eg = warp_sum_ll(eg);
+    if ((threadIdx.x & 31) == 0) energy_add(x, MDN_U_GAS, eg);
+  }
+}
+
+/* near molecules: one warp each; gas-ion and gas-vapor lists; the molecule's
+ * own force is reduced over the warp, the reaction goes to the core sums */
+__device__ void gas_near_pass(Ctx& x, bool eflag, bool kick) {
+  const RepParams* P = x.P;
+  const KArgs* a = x.a;
+  const int ag = P->a_g, av = P->a_v, par = x.D->parity, nt = P->n_types, ni = P->n_ion;
+  const bool gi = term_on(x, MDN_I_GI), gv = term_on(x, MDN_I_GV);
+  const bool intra = term_on(x, MDN_I_GAS_INTRA) && P->n_gas_bonds > 0;
+  const int nj = (P->quirks & MDN_Q_GV_GAS_COUNT) ? min(ag, av) : av;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int lo, hi;
+  partition(x, x.D->n_gas_in, &lo, &hi);
+  /* this CTA's range of the (ascending) near list */
+  const int* nl = a->near_list + P->near_off;
+  const int nn = x.D->n_near;
+  int b0 = 0, b1 = nn;
+  {
+    int L = 0, H = nn;
+    while (L < H) { int M = (L + H) >> 1; if (nl[M] < lo) L = M + 1; else H = M; }
+    b0 = L;
+    L = b0; H = nn;
+    while (L < H) { int M = (L + H) >> 1; if (nl[M] < hi) L = M + 1; else H = M; }
+    b1 = L;
+  }
+  int gtype[MDN_MAX_GAS_ATOMS];
+  double c2[MDN_MAX_GAS_ATOMS];
+  for (int at = 0; at < ag; at++) {
+    gtype[at] = x.ib[P->o_gas_type + at];
+    c2[at] = x.c.c2[gtype[at]];
+  }
+  const double* com = x.D->ion_com;
+  long long egi = 0, egv = 0, eintra = 0;
+  for (int e = b0 + wid; e < b1; e += nw) {
+    const int s = nl[e];
+    const size_t ms = gmol(P, par, s);
+    float3 gp[MDN_MAX_GAS_ATOMS];
+    double X[3 * MDN_MAX_GAS_ATOMS];
+    for (int at = 0; at < ag; at++) {
+      size_t g = gatom(P, par, s, at);
+      for (int k = 0; k < 3; k++) X[3 * at + k] = a->slab_x[3 * g + k];
+      gp[at] = make_float3((float)(X[3 * at] - com[0]), (float)(X[3 * at + 1] - com[1]),
+                           (float)(X[3 * at + 2] - com[2]));
+    }
+    long long F[MDN_MAX_GAS_ATOMS][3];
+    for (int at = 0; at < MDN_MAX_GAS_ATOMS; at++) F[at][0] = F[at][1] = F[at][2] = 0;
+    if (gi) {
+      const int start = a->near_gi[ms], cnt = a->gil_n[ms];
+      for (int q = lane; q < cnt; q += 32) {
+        int j = a->gil[P->gil_off + start + q];
+        float4 pj = x.c.pos[j];
+        int tj = x.c.type[j];
+        long long R[3] = {0, 0, 0};
+        for (int at = 0; at < ag; at++) {
+          float dx = gp[at].x - pj.x, dy = gp[at].y - pj.y, dz = gp[at].z - pj.z;
+          float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+          float ee;
+          float fp = lj_coul(r2, x.c.ljA[gtype[at] * nt + tj], x.c.ljB[gtype[at] * nt + tj], 0.0f, false, &ee);
+          long long fx = fixf(fp * dx), fy = fixf(fp * dy), fz = fixf(fp * dz);
+          F[at][0] += fx; F[at][1] += fy; F[at][2] += fz;
+          R[0] -= fx; R[1] -= fy; R[2] -= fz;
+          if (eflag)
+            egi += efixd(lj_coul_energy(r2d(X + 3 * at, x.c.x + 3 * j), x.db[P->d_ljA + gtype[at] * nt + tj],
+                                        x.db[P->d_ljB + gtype[at] * nt + tj], 0.0));
+        }
+        acc_add(x, j, R);
+      }
+    }
+    if (gv) {
+      const int start = a->near_gv[ms], cnt = a->gvl_n[ms];
+      const int tot = cnt * nj;
+      for (int q = lane; q < tot; q += 32) {
+        int ent = q / nj, b = q - ent * nj;
+        int vs = a->gvl[P->gvl_off + start + ent];
+        int j = ni + vs * av + b;
+        float4 pj = x.c.pos[j];
+        int tj = x.c.type[j];
+        long long R[3] = {0, 0, 0};
+        for (int at = 0; at < ag; at++) {
+          float dx = gp[at].x - pj.x, dy = gp[at].y - pj.y, dz = gp[at].z - pj.z;
+          float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+          float ee;
+          float fp = lj_coul(r2, x.c.ljA[gtype[at] * nt + tj], x.c.ljB[gtype[at] * nt + tj], 0.0f, false, &ee);
+          long long fx = fixf(fp * dx), fy = fixf(fp * dy), fz = fixf(fp * dz);
+          F[at][0] += fx; F[at][1] += fy; F[at][2] += fz;
+          R[0] -= fx; R[1] -= fy; R[2] -= fz;
+          if (eflag)
+            egv += efixd(lj_coul_energy(r2d(X + 3 * at, x.c.x + 3 * j), x.db[P->d_ljA + gtype[at] * nt + tj],
+                                        x.db[P->d_ljB + gtype[at] * nt + tj], 0.0));
+        }
+        acc_add(x, j, R);
+      }
+    }
+    for (int at = 0; at < ag; at++)
+      for (int k = 0; k < 3; k++) F[at][k] = warp_sum_ll(F[at][k]);
+    if (lane == 0) {
+      double Fd[3 * MDN_MAX_GAS_ATOMS];
+      for (int at = 0; at < ag; at++)
+        for (int k = 0; k < 3; k++) Fd[3 * at + k] = (double)F[at][k] * MDN_FIX_INV;
+      if (intra) {
+        double ei = gas_intra(x, X, Fd);
+        if (eflag) eintra += efixd(ei);
+      }
+      for (int at = 0; at < ag; at++) {
+        size_t g = gatom(P, par, s, at);
+        for (int k = 0; k < 3; k++) {
+          if (kick) a->slab_v[3 * g + k] += Fd[3 * at + k] * c2[at];
+          a->slab_f[3 * g + k] = Fd[3 * at + k];
+        }
+      }
+    }
+  }
+  if (eflag) {
+    egi = warp_sum_ll(egi);
+    egv = warp_sum_ll(egv);
+    if (lane == 0) {
+      energy_add(x, MDN_U_GI, egi);
+      energy_add(x, MDN_U_VG, egv);
+      energy_add(x, MDN_U_GAS, eintra);
+    }
+  }
+}
+
+/* sum of the core partials over the cluster -> f (double), identical in every CTA */
+__device__ void core_reduce(Ctx& x, cg::cluster_group& cl) {
+  const int n3 = 3 * x.n_core;
+  long long* mine = x.c.acc + (size_t)x.buf * 3 * x.a->nc_cap;
+  if (x.C > 1) {
+    cl.sync();
+    for (int q = threadIdx.x; q < n3; q += blockDim.x) {
+      long long s = 0;
+      for (int k = 0; k < x.C; k++) {
+        const long long* other = cl.map_shared_rank(mine, k);
+        s += other[q];
+      }
+      x.c.f[q] = (double)s * MDN_FIX_INV;
+    }
+  } else {
+    for (int q = threadIdx.x; q < n3; q += blockDim.x) x.c.f[q] = (double)mine[q] * MDN_FIX_INV;
+  }
+  __syncthreads();
+  /* flag forces outside the fixed-point range or non-finite */
+  if (x.rank == 0)
+    for (int q = threadIdx.x; q < n3; q += blockDim.x) {
+      double f = x.c.f[q];
+      if (!(fabs(f) < MDN_FIX_LIMIT)) set_status(x, MDN_ST_FIXED_OVERFLOW);
+    }
+  x.buf ^= 1;  /* the next evaluation accumulates into the other buffer */
+}
+
+__device__ void zero_acc(Ctx& x) {
+  long long* mine = x.c.acc + (size_t)x.buf * 3 * x.a->nc_cap;
+  for (int q = threadIdx.x; q < 3 * x.n_core; q += blockDim.x) mine[q] = 0;
+  __syncthreads();
+}
+
+/* all forces of the step (after positions and lists are final) and the second kick */
+__device__ void forces_and_kick(Ctx& x, cg::cluster_group& cl, bool eflag, bool kick) {
+  zero_acc(x);
+  gas_near_pass(x, eflag, kick);
+  core_bonded(x, eflag);
+  core_pairs(x, eflag);
+  __syncthreads();
+  core_reduce(x, cl);
+  if (kick) {
+    core_kick(x);
+    __syncthreads();
+  }
+}
+
+/* ------------------------------------------------------------------------- */
+/* the effective-domain rebuild (MD::make_pair)                               */
+/* ------------------------------------------------------------------------- */
+__device__ void insert_gas(const Ctx& x, int q, int n_rebuild, double* X, double* V) {
+  const RepParams* P = x.P;
+  const int ag = P->a_g, mi = 1 + q;
+  const double* cx = x.a->mol_x + 3 * ((size_t)P->mol_off + mi);
+  const double* cv = x.a->mol_v + 3 * ((size_t)P->mol_off + mi);
+  for (int at = 0; at < ag; at++)
+    for (int k = 0; k < 3; k++) {
+      X[3 * at + k] = x.db[P->d_gas_x + 3 * at + k];
+      V[3 * at + k] = 0;
+    }
+  if (P->gas_kind == MDN_GAS_N2 && ag == 2) {
+    U4 s = draw(*P, mi, n_rebuild, 1, 1);
+    double vy, vz;
+    box_muller(s.v[0], s.v[1], vy, vz);
+    vy *= P->gas_sigma;
+    vz *= P->gas_sigma;
+    double vzu = (P->quirks & MDN_Q_N2_ROT_VYVZ) ? vy : vz;
+    V[0] = 0; V[1] = vy; V[2] = vzu;
+    V[3] = 0; V[4] = -vy; V[5] = -vzu;
+  }
+  U4 s = draw(*P, mi, n_rebuild, 1, 0);
+  double A = u01(s.v[0]) * 2 * 3.141592653589793;
+  double B = u01(s.v[1]) * 2 * 3.141592653589793;
+  double Cc = u01(s.v[2]) * 2 * 3.141592653589793;
+  const bool zy = (P->quirks & MDN_Q_GAS_ROT_ZY) != 0;
+  for (int at = 0; at < ag; at++) {
+    double* p = X + 3 * at;
+    rotation(p[0], p[1], p[2], A, B, Cc, p[0], p[1], zy ? p[1] : p[2]);
+    for (int k = 0; k < 3; k++) p[k] += cx[k];
+  }
+  for (int at = 0; at < ag; at++) {
+    double* p = V + 3 * at;
+    rotation(p[0], p[1], p[2], A, B, Cc, p[0], p[1], zy ? p[1] : p[2]);
+    for (int k = 0; k < 3; k++) p[k] += cv[k];
+  }
+}
+
+__device__ void insert_vapor(const Ctx& x, int q, int n_rebuild, double* X, double* V) {
+  const RepParams* P = x.P;
+  const int av = P->a_v, mi = 1 + P->n_gas + q;
+  const double* cx = x.a->mol_x + 3 * ((size_t)P->mol_off + mi);
+  const double* cv = x.a->mol_v + 3 * ((size_t)P->mol_off + mi);
+  U4 s = draw(*P, mi, n_rebuild, 1, 0);
+  double A = u01(s.v[0]) * 2 * 3.141592653589793;
+  double B = u01(s.v[1]) * 2 * 3.141592653589793;
+  double Cc = u01(s.v[2]) * 2 * 3.141592653589793;
+  for (int at = 0; at < av; at++) {
+    double* p = X + 3 * at;
+    for (int k = 0; k < 3; k++) p[k] = x.db[P->d_vap_x + 3 * at + k];
+    rotation(p[0], p[1], p[2], A, B, Cc, p[0], p[1], p[2]);
+    for (int k = 0; k < 3; k++) p[k] += cx[k];
+    double* u = V + 3 * at;
+    u[0] = u[1] = u[2] = 0;
+    rotation(u[0], u[1], u[2], A, B, Cc, u[0], u[1], u[2]);
+    for (int k = 0; k < 3; k++) u[k] += cv[k];
+  }
+}
+
+/* free flight, in/out test, wrap and resampling of one molecule; returns
+ * (was_in << 1) | now_in */
+__device__ __forceinline__ int classify_one(const Ctx& x, int mi, double sigma, int n_rebuild, int loop_pair,
+                                            const double* com) {
+  const RepParams* P = x.P;
+  const size_t g = (size_t)P->mol_off + mi;
+  double* X = x.a->mol_x + 3 * g;
+  double* V = x.a->mol_v + 3 * g;
+  const int was = x.a->region[g] & 1;
+  if (!was)
+    for (int k = 0; k < 3; k++) X[k] += V[k] * P->dt * loop_pair;
+  double dx = X[0] - com[0];
+  double dy = X[1] - com[1];
+  double dz = X[2] - com[2];
+  double r2 = (dx * dx + dy * dy + dz * dz);
+  int in = r2 < P->RI2 ? 1 : 0;
+  if (!in) {
+    double HL = P->box * 0.5;
+    if (dx < -HL) X[0] += P->box;
+    if (dy < -HL) X[1] += P->box;
+    if (dz < -HL) X[2] += P->box;
+    if (dx > HL) X[0] -= P->box;
+    if (dy > HL) X[1] -= P->box;
+    if (dz > HL) X[2] -= P->box;
+    U4 s = draw(*P, mi, n_rebuild, 0, 0);
+    double z0, z1, z2, z3;
+    box_muller(s.v[0], s.v[1], z0, z1);
+    box_muller(s.v[2], s.v[3], z2, z3);
+    V[0] = z0 * sigma;
+    V[1] = z1 * sigma;
+    V[2] = z2 * sigma;
+  }
+  x.a->region[g] = (unsigned char)((was << 1) | in);
+  return (was << 1) | in;
+}
+
+/* exchange one int per CTA across the cluster: returns the prefix before this
+ * rank and the total */
+__device__ void cluster_prefix(Ctx& x, cg::cluster_group& cl, int* slot_in_smem, int mine, int* before,
+                               int* total) {
+  if (threadIdx.x == 0) *slot_in_smem = mine;
+  cl.sync();
+  int b = 0, t = 0;
+  for (int k = 0; k < x.C; k++) {
+    int v = *cl.map_shared_rank(slot_in_smem, k);
+    if (k < x.rank) b += v;
+    t += v;
+  }
+  *before = b;
+  *total = t;
+  cl.sync();
+}
+
+/* pair lists of the gas slab (current parity) from the centres: gas-ion
+ * (PotentialGasIon::makePair) and gas-vapor (PotentialVaporGas::makePair) */
+__device__ void relist(Ctx& x, cg::cluster_group& cl) {
+  const RepParams* P = x.P;
+  const KArgs* a = x.a;
+  const int par = x.D->parity, ni = P->n_ion, nv = x.D->n_vap_in;
+  const bool gi = (P->interactions & MDN_I_GI) != 0, gv = (P->interactions & MDN_I_GV) != 0;
+  int lo, hi;
+  partition(x, x.D->n_gas_in, &lo, &hi);
+  /* bounding sphere of the ion, exact test below */
+  int* sc = x.iscr;
+  int gi_tot = 0, gv_tot = 0, nn_tot = 0;
+  int gi_base = 0, gv_base = 0, nn_base = 0;
+  /* pass 1: counts */
+  int my_gi = 0, my_gv = 0, my_nn = 0;
+  for (int s0 = lo; s0 < hi; s0 += blockDim.x) {
+    int s = s0 + threadIdx.x;
+    int cgi = 0, cgv = 0;
+    if (s < hi) {
+      int m = a->slab_mol[gmol(P, par, s)];
+      const double* cm = a->mol_x + 3 * ((size_t)P->mol_off + 1 + m);
+      if (gi)
+        for (int j = 0; j < ni; j++) {
+          double dx = cm[0] - x.c.x[3 * j], dy = cm[1] - x.c.x[3 * j + 1], dz = cm[2] - x.c.x[3 * j + 2];
+          if ((dx * dx + dy * dy + dz * dz) < P->ml2) cgi++;
+        }
+      if (gv)
+        for (int q = 0; q < nv; q++) {
+          int vm = a->vslab_mol[vmol(P, par, q)];
+          const double* vc = a->mol_x + 3 * ((size_t)P->mol_off + 1 + P->n_gas + vm);
+          double dx = cm[0] - vc[0], dy = cm[1] - vc[1], dz = cm[2] - vc[2];
+          if ((dx * dx + dy * dy + dz * dz) < P->ml2) cgv++;
+        }
+    }
+    my_gi += cgi;
+    my_gv += cgv;
+    my_nn += (cgi + cgv) > 0 ? 1 : 0;
+  }
+  my_gi = block_sum_i(my_gi, sc);
+  my_gv = block_sum_i(my_gv, sc);
+  my_nn = block_sum_i(my_nn, sc);
+  cluster_prefix(x, cl, &sc[40], my_gi, &gi_base, &gi_tot);
+  cluster_prefix(x, cl, &sc[41], my_gv, &gv_base, &gv_tot);
+  cluster_prefix(x, cl, &sc[42], my_nn, &nn_base, &nn_tot);
+  bool over = gi_tot > P->gil_cap || gv_tot > P->gvl_cap || nn_tot > P->near_cap;
+  if (over && threadIdx.x == 0 && x.rank == 0) set_status(x, MDN_ST_LIST_OVERFLOW);
+  /* pass 2: fill, ascending slab slot */
+  int run_gi = gi_base, run_gv = gv_base, run_nn = nn_base;
+  for (int s0 = lo; s0 < hi; s0 += blockDim.x) {
+    int s = s0 + threadIdx.x;
+    int cgi = 0, cgv = 0;
+    const double* cm = nullptr;
+    if (s < hi) {
+      int m = a->slab_mol[gmol(P, par, s)];
+      cm = a->mol_x + 3 * ((size_t)P->mol_off + 1 + m);
+      if (gi)
+        for (int j = 0; j < ni; j++) {
+          double dx = cm[0] - x.c.x[3 * j], dy = cm[1] - x.c.x[3 * j + 1], dz = cm[2] - x.c.x[3 * j + 2];
+          if ((dx * dx + dy * dy + dz * dz) < P->ml2) cgi++;
+        }
+      if (gv)
+        for (int q = 0; q < nv; q++) {
+          int vm = a->vslab_mol[vmol(P, par, q)];
+          const double* vc = a->mol_x + 3 * ((size_t)P->mol_off + 1 + P->n_gas + vm);
+          double dx = cm[0] - vc[0], dy = cm[1] - vc[1], dz = cm[2] - vc[2];
+          if ((dx * dx + dy * dy + dz * dz) < P->ml2) cgv++;
+        }
+    }
+    int t_gi, t_gv, t_nn;
+    int o_gi = block_exscan(cgi, sc, &t_gi);
+    int o_gv = block_exscan(cgv, sc, &t_gv);
+    int isn = (cgi + cgv) > 0 ? 1 : 0;
+    int o_nn = block_exscan(isn, sc, &t_nn);
+    if (s < hi) {
+      size_t ms = gmol(P, par, s);
+      if (isn && !over) {
+        int bgi = run_gi + o_gi, bgv = run_gv + o_gv;
+        a->near_list[P->near_off + run_nn + o_nn] = s;
+        a->near_gi[ms] = bgi;
+        a->near_gv[ms] = bgv;
+        a->gil_n[ms] = (unsigned short)cgi;
+        a->gvl_n[ms] = (unsigned short)cgv;
+        int w = 0;
+        if (gi)
+          for (int j = 0; j < ni; j++) {
+            double dx = cm[0] - x.c.x[3 * j], dy = cm[1] - x.c.x[3 * j + 1], dz = cm[2] - x.c.x[3 * j + 2];
+            if ((dx * dx + dy * dy + dz * dz) < P->ml2) a->gil[P->gil_off + bgi + w++] = (unsigned short)j;
+          }
+        w = 0;
+        if (gv)
+          for (int q = 0; q < nv; q++) {
+            int vm = a->vslab_mol[vmol(P, par, q)];
+            const double* vc = a->mol_x + 3 * ((size_t)P->mol_off + 1 + P->n_gas + vm);
+            double dx = cm[0] - vc[0], dy = cm[1] - vc[1], dz = cm[2] - vc[2];
+            if ((dx * dx + dy * dy + dz * dz) < P->ml2) a->gvl[P->gvl_off + bgv + w++] = (unsigned short)q;
+          }
+      } else {
+        a->near_gi[ms] = -1;
+        a->near_gv[ms] = -1;
+        a->gil_n[ms] = 0;
+        a->gvl_n[ms] = 0;
+      }
+    }
+    run_gi += t_gi;
+    run_gv += t_gv;
+    run_nn += t_nn;
+  }
+  if (threadIdx.x == 0) {
+    x.D->gi_count = over ? 0 : gi_tot;
+    x.D->gv_count = over ? 0 : gv_tot;
+    x.D->n_near = over ? 0 : nn_tot;
+  }
+  __threadfence();
+  cl.sync();
+}
+
+__device__ void make_pair(Ctx& x, cg::cluster_group& cl) {
+  const RepParams* P = x.P;
+  const KArgs* a = x.a;
+  const int ag = P->a_g, av = P->a_v, par = x.D->parity, npar = par ^ 1;
+  const int loop_pair = x.D->loop_pair, nreb = x.D->n_rebuilds;
+  int* sc = x.iscr;
+  /* updateInCenters: gas slab partition of this CTA, vapor core by rank 0 */
+  {
+    int lo, hi;
+    partition(x, x.D->n_gas_in, &lo, &hi);
+    for (int s = lo + threadIdx.x; s < hi; s += blockDim.x) {
+      int m = a->slab_mol[gmol(P, par, s)];
+      double sx[3] = {0, 0, 0}, sv[3] = {0, 0, 0};
+      for (int at = 0; at < ag; at++) {
+        size_t g = gatom(P, par, s, at);
+        double mm = x.db[P->d_mass + x.ib[P->o_gas_type + at]];
+        for (int k = 0; k < 3; k++) {
+          sx[k] += a->slab_x[3 * g + k] * mm;
+          sv[k] += a->slab_v[3 * g + k] * mm;
+        }
+      }
+      double massInv = 1 / P->gas_com_mass;
+      size_t g = (size_t)P->mol_off + 1 + m;
+      for (int k = 0; k < 3; k++) {
+        a->mol_x[3 * g + k] = sx[k] * massInv;
+        a->mol_v[3 * g + k] = sv[k] * massInv;
+      }
+    }
+    if (x.rank == 0)
+      for (int s = threadIdx.x; s < x.D->n_vap_in; s += blockDim.x) {
+        int m = a->vslab_mol[vmol(P, par, s)];
+        double sx[3] = {0, 0, 0}, sv[3] = {0, 0, 0};
+        for (int at = 0; at < av; at++) {
+          int i = P->n_ion + s * av + at;
+          double mm = x.db[P->d_mass + x.c.type[i]];
+          for (int k = 0; k < 3; k++) {
+            sx[k] += x.c.x[3 * i + k] * mm;
+            sv[k] += x.c.v[3 * i + k] * mm;
+          }
+        }
+        double massInv = 1 / P->vap_com_mass;
+        size_t g = (size_t)P->mol_off + 1 + P->n_gas + m;
+        for (int k = 0; k < 3; k++) {
+          a->mol_x[3 * g + k] = sx[k] * massInv;
+          a->mol_v[3 * g + k] = sv[k] * massInv;
+        }
+      }
+  }
+  /* the ion centre in the reference's summation order (MD::update_position
+   * computed it just before check_pairlist); MD::MD's first make_pair and the
+   * re-centring in MD::run use the stored entry instead */
+  if (!a->keep_com) ion_centre_exact(x);
+  if (x.rank == 0 && threadIdx.x == 0) {
+    size_t g = (size_t)P->mol_off;
+    for (int k = 0; k < 3; k++) {
+      a->mol_x[3 * g + k] = x.D->ion_com[k];
+      a->mol_v[3 * g + k] = x.D->ion_com[3 + k];
+    }
+  }
+  __threadfence();
+  cl.sync();
+  /* free flight + classification of the gas molecules of this CTA's range */
+  double com[3] = {x.D->ion_com[0], x.D->ion_com[1], x.D->ion_com[2]};
+  int mlo, mhi;
+  partition(x, P->n_gas, &mlo, &mhi);
+  int my_in = 0;
+  double vmax2 = 0;
+  for (int q = mlo + threadIdx.x; q < mhi; q += blockDim.x) {
+    int f = classify_one(x, 1 + q, P->gas_sigma, nreb, loop_pair, com);
+    my_in += f & 1;
+    const double* V = a->mol_v + 3 * ((size_t)P->mol_off + 1 + q);
+    double v2 = V[0] * V[0] + V[1] * V[1] + V[2] * V[2];
+    vmax2 = fmax(vmax2, v2);
+  }
+  /* vapor molecules (rank 0; events) */
+  int my_vin = 0;
+  if (x.rank == 0)
+    for (int q = threadIdx.x; q < P->n_vap; q += blockDim.x) {
+      int mi = 1 + P->n_gas + q;
+      size_t g = (size_t)P->mol_off + mi;
+      int was = a->region[g] & 1;
+      if (was) {
+        /* MD::Ovin / MD::Ovout log the centre before any change */
+        double dx[3], dv[3];
+        for (int k = 0; k < 3; k++) {
+          dx[k] = a->mol_x[3 * g + k] - com[k];
+          dv[k] = a->mol_v[3 * g + k] - x.D->ion_com[3 + k];
+        }
+        double r2 = dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2];
+        int e = atomicAdd(a->n_events, 1);
+        if (e < a->ev_cap) {
+          DevEvent& ev = a->events[e];
+          ev.replica = x.r;
+          ev.molecule = q;
+          ev.kind = r2 < P->RI2 ? 1 : 2;
+          ev.step = x.D->step;
+          for (int k = 0; k < 3; k++) { ev.dx[k] = dx[k]; ev.dv[k] = dv[k]; }
+        } else {
+          set_status(x, MDN_ST_EVENT_OVERFLOW);
+        }
+      }
+      int f = classify_one(x, mi, P->vap_sigma, nreb, loop_pair, com);
+      my_vin += f & 1;
+      const double* V = a->mol_v + 3 * g;
+      double v2 = V[0] * V[0] + V[1] * V[1] + V[2] * V[2];
+      vmax2 = fmax(vmax2, v2);
+    }
+  {
+    const double* V = x.D->ion_com + 3;
+    vmax2 = fmax(vmax2, V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
+  }
+  my_in = block_sum_i(my_in, sc);
+  my_vin = block_sum_i(my_vin, sc);
+  vmax2 = block_max_d(vmax2, x.dscr);
+  __threadfence();
+  int gin_base, gin_tot, vin_base, vin_tot;
+  cluster_prefix(x, cl, &sc[43], my_in, &gin_base, &gin_tot);
+  cluster_prefix(x, cl, &sc[44], my_vin, &vin_base, &vin_tot);
+  /* vmax over the cluster */
+  if (threadIdx.x == 0) x.dscr[45] = vmax2;
+  cl.sync();
+  double vm2 = 0;
+  for (int k = 0; k < x.C; k++) vm2 = fmax(vm2, *cl.map_shared_rank(&x.dscr[45], k));
+  cl.sync();
+  const bool slab_over = gin_tot > P->slab_cap;
+  const bool core_over = vin_tot > P->vcap || P->n_ion + vin_tot * av > a->nc_cap;
+  /* new gas slab, ascending molecule index */
+  int run = gin_base;
+  for (int q0 = mlo; q0 < mhi; q0 += blockDim.x) {
+    int q = q0 + threadIdx.x;
+    int f = 0;
+    if (q < mhi) f = a->region[(size_t)P->mol_off + 1 + q];
+    int in = f & 1, tot;
+    int off = block_exscan(in, sc, &tot);
+    if (q < mhi) {
+      size_t g = (size_t)P->mol_off + 1 + q;
+      if (in && !slab_over) {
+        int ns = run + off;
+        double X[3 * MDN_MAX_GAS_ATOMS], V[3 * MDN_MAX_GAS_ATOMS];
+        if (f & 2) {
+          int os = a->slot[g];
+          for (int at = 0; at < ag; at++) {
+            size_t go = gatom(P, par, os, at);
+            for (int k = 0; k < 3; k++) {
+              X[3 * at + k] = a->slab_x[3 * go + k];
+              V[3 * at + k] = a->slab_v[3 * go + k];
+            }
+          }
+        } else {
+          insert_gas(x, q, nreb, X, V);
+        }
+        for (int at = 0; at < ag; at++) {
+          size_t gn = gatom(P, npar, ns, at);
+          for (int k = 0; k < 3; k++) {
+            a->slab_x[3 * gn + k] = X[3 * at + k];
+            a->slab_v[3 * gn + k] = V[3 * at + k];
+            a->slab_f[3 * gn + k] = 0.0;
+          }
+        }
+        a->slab_mol[gmol(P, npar, ns)] = q;
+        a->slot[g] = ns;
+      } else {
+        a->slot[g] = -1;
+      }
+      a->region[g] = (unsigned char)in;
+    }
+    run += tot;
+  }
+  /* new vapor slab (rank 0), from the core copy (current positions); each
+   * molecule reads its own old slot before overwriting it */
+  if (x.rank == 0) {
+    int runv = 0;
+    for (int q0 = 0; q0 < P->n_vap; q0 += blockDim.x) {
+      int q = q0 + threadIdx.x;
+      int f = 0;
+      if (q < P->n_vap) f = a->region[(size_t)P->mol_off + 1 + P->n_gas + q];
+      int in = f & 1, tot;
+      int off = block_exscan(in, sc, &tot);
+      if (q < P->n_vap) {
+        size_t g = (size_t)P->mol_off + 1 + P->n_gas + q;
+        if (in && !core_over) {
+          int ns = runv + off;
+          double X[3 * MDN_MAX_VAP_ATOMS], V[3 * MDN_MAX_VAP_ATOMS];
+          if (f & 2) {
+            int os = a->slot[g];
+            for (int at = 0; at < av; at++) {
+              int i = P->n_ion + os * av + at;
+              for (int k = 0; k < 3; k++) {
+                X[3 * at + k] = x.c.x[3 * i + k];
+                V[3 * at + k] = x.c.v[3 * i + k];
+              }
+            }
+          } else {
+            insert_vapor(x, q, nreb, X, V);
+          }
+          for (int at = 0; at < av; at++) {
+            size_t gn = vatom(P, npar, ns, at);
+            for (int k = 0; k < 3; k++) {
+              a->vslab_x[3 * gn + k] = X[3 * at + k];
+              a->vslab_v[3 * gn + k] = V[3 * at + k];
+              a->vslab_f[3 * gn + k] = 0.0;
+            }
+            a->vslab_w[gn] = (f & 2) ? 0.0f : -1.0f;
+          }
+          a->vslab_mol[vmol(P, npar, ns)] = q;
+          a->slot[g] = ns;
+        } else {
+          a->slot[g] = -1;
+        }
+        a->region[g] = (unsigned char)in;
+      }
+      runv += tot;
+    }
+  }
+  __threadfence();
+  cl.sync();
+  /* new counters, identical in every CTA */
+  if (threadIdx.x == 0) {
+    if (slab_over && x.rank == 0) set_status(x, MDN_ST_SLAB_OVERFLOW);
+    if (core_over && x.rank == 0) set_status(x, MDN_ST_CORE_OVERFLOW);
+    x.D->parity = npar;
+    x.D->n_gas_in = slab_over ? 0 : gin_tot;
+    x.D->n_vap_in = core_over ? 0 : vin_tot;
+    double vmax = sqrt(vm2);
+    double lu = x.D->margin_length / (vmax * P->dt);
+    x.D->loop_update = lu >= 2147483647.0 ? 2147483647 : (int)lu;
+    x.D->loop_pair = 0;
+    x.D->n_rebuilds = nreb + 1;
+  }
+  __syncthreads();
+  /* reload the vapor part of the core from the new vapor slab */
+  load_vapor(x);
+  __syncthreads();
+  core_weights_pos(x, true);
+  relist(x, cl);
+}
+
+/* ------------------------------------------------------------------------- */
+__device__ void one_step(Ctx& x, cg::cluster_group& cl, bool eflag) {
+  const RepParams* P = x.P;
+  core_kick(x);
+  __syncthreads();
+  if (x.D->nvt_mode == MDN_NVT_SCALE) {
+    double T = ion_temperature(x);
+    double ratio = sqrt(300.0 / T);
+    for (int i = threadIdx.x; i < P->n_ion; i += blockDim.x)
+      for (int k = 0; k < 3; k++) x.c.v[3 * i + k] *= ratio;
+    __syncthreads();
+  }
+  core_drift_shake(x);
+  ion_centre(x);
+  if (x.D->nvt_mode == MDN_NVT_NH) {
+    double T = ion_temperature(x);
+    if (threadIdx.x == 0) {
+      int g = P->n_ion * 3;
+      x.D->zeta += (T - x.D->nvt_T) * g * P->kb_real * 0.0001 * P->dt;
+    }
+    __syncthreads();
+  }
+  core_weights_pos(x, true);
+  const bool rebuild = x.D->loop_pair + 1 > x.D->loop_update;
+  gas_integrate(x, !rebuild, eflag);
+  __threadfence_block();
+  __syncthreads();
+  if (threadIdx.x == 0) x.D->loop_pair += 1;
+  __syncthreads();
+  if (rebuild) {
+    make_pair(x, cl);
+    gas_far_pass(x, eflag, true);
+    __syncthreads();
+  }
+  forces_and_kick(x, cl, eflag, true);
+  if (x.D->nvt_mode == MDN_NVT_NH) {
+    double Coeff = exp(-x.D->zeta * 0.5 * P->dt);
+    for (int i = threadIdx.x; i < P->n_ion; i += blockDim.x)
+      for (int k = 0; k < 3; k++) x.c.v[3 * i + k] *= Coeff;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) x.D->step += 1;
+  __syncthreads();
+}
+
+}  // namespace
+
+extern "C" __global__ void __launch_bounds__(512, 1) mdn_advance(KArgs a) {
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ __align__(16) unsigned char dsm[];
+  __shared__ RepParams sP;
+  __shared__ RepDyn sD;
+  __shared__ int s_job;
+  __shared__ int iscr[64];
+  __shared__ double dscr[64];
+
+  Ctx x;
+  x.a = &a;
+  x.P = &sP;
+  x.D = &sD;
+  x.rank = (int)cl.block_rank();
+  x.C = (int)cl.num_blocks();
+  x.iscr = iscr;
+  x.dscr = dscr;
+  /* carve the dynamic shared memory */
+  {
+    unsigned char* p = dsm;
+    const int nc = a.nc_cap;
+    auto take = [&](size_t bytes) { unsigned char* q = p; p += (bytes + 15) & ~(size_t)15; return q; };
+    x.c.acc = (long long*)take(sizeof(long long) * 6 * nc);
+    x.c.x = (double*)take(sizeof(double) * 3 * nc);
+    x.c.v = (double*)take(sizeof(double) * 3 * nc);
+    x.c.f = (double*)take(sizeof(double) * 3 * nc);
+    x.c.xold = (double*)take(sizeof(double) * 3 * nc);
+    x.c.pos = (float4*)take(sizeof(float4) * nc);
+    x.c.w = (float*)take(sizeof(float) * nc);
+    x.c.type = (int*)take(sizeof(int) * nc);
+    x.c.mol = (int*)take(sizeof(int) * nc);
+    x.c.excl = (unsigned*)take(sizeof(unsigned) * a.excl_cap);
+    x.c.ljA = (float*)take(sizeof(float) * a.nt_cap * a.nt_cap);
+    x.c.ljB = (float*)take(sizeof(float) * a.nt_cap * a.nt_cap);
+    x.c.c2 = (double*)take(sizeof(double) * a.nt_cap);
+  }
+  x.buf = 0;
+  for (;;) {
+    if (x.rank == 0 && threadIdx.x == 0) s_job = atomicAdd(a.job_counter, 1);
+    cl.sync();
+    const int job = *cl.map_shared_rank(&s_job, 0);
+    cl.sync();
+    if (job >= a.n_jobs) break;
+    const int r = a.job_order[job];
+    x.r = r;
+    if (threadIdx.x == 0) {
+      sP = a.P[r];
+      sD = a.D[r];
+    }
+    __syncthreads();
+    x.ib = a.iblob + sP.iblob_off;
+    x.db = a.dblob + sP.dblob_off;
+    const bool fatal =
+        (a.status[r] & (MDN_ST_SLAB_OVERFLOW | MDN_ST_CORE_OVERFLOW | MDN_ST_LIST_OVERFLOW)) != 0;
+    const bool fits = sP.n_types <= a.nt_cap && sP.n_ion * sP.excl_words <= a.excl_cap &&
+                      sP.n_ion + sD.n_vap_in * sP.a_v <= a.nc_cap;
+    if (fatal || !fits) {
+      if (!fits && x.rank == 0 && threadIdx.x == 0) atomicOr(&a.status[r], MDN_ST_CORE_OVERFLOW);
+      __syncthreads();
+      continue;
+    }
+    /* tables */
+    const int nt = sP.n_types;
+    for (int q = threadIdx.x; q < nt * nt; q += blockDim.x) {
+      x.c.ljA[q] = (float)x.db[sP.d_ljA + q];
+      x.c.ljB[q] = (float)x.db[sP.d_ljB + q];
+    }
+    for (int q = threadIdx.x; q < nt; q += blockDim.x) x.c.c2[q] = x.db[sP.d_c2 + q];
+    for (int q = threadIdx.x; q < sP.n_ion * sP.excl_words; q += blockDim.x) x.c.excl[q] = (unsigned)x.ib[sP.o_excl + q];
+    load_ion(x);
+    load_vapor(x);
+    __syncthreads();
+    if (a.mode == MDN_MODE_STEP) {
+      for (long long s = 0; s < a.n_steps; s++) {
+        bool eflag = a.energy_mode == 2 || (a.energy_mode == 1 && s == a.n_steps - 1);
+        one_step(x, cl, eflag);
+      }
+    } else if (a.mode == MDN_MODE_FORCES) {
+      /* the ion centre serves only as the origin of the FP32 coordinates here */
+      double keep[6];
+      for (int k = 0; k < 6; k++) keep[k] = sD.ion_com[k];
+      __syncthreads();
+      ion_centre(x);
+      core_weights_pos(x, false);
+      gas_far_pass(x, true, false);
+      __syncthreads();
+      forces_and_kick(x, cl, true, false);
+      if (threadIdx.x == 0)
+        for (int k = 0; k < 6; k++) sD.ion_com[k] = keep[k];
+      __syncthreads();
+    } else if (a.mode == MDN_MODE_MAKE_PAIR) {
+      core_weights_pos(x, false);
+      make_pair(x, cl);
+    } else if (a.mode == MDN_MODE_RELIST) {
+      relist(x, cl);
+    }
+    __syncthreads();
+    store_core(x);
+    __syncthreads();
+    if (x.rank == 0 && threadIdx.x == 0) {
+      a.D[r] = sD;
+      if (a.mode == MDN_MODE_STEP) {
+        size_t g = (size_t)sP.mol_off;
+        for (int k = 0; k < 3; k++) {
+          a.mol_x[3 * g + k] = sD.ion_com[k];
+          a.mol_v[3 * g + k] = sD.ion_com[3 + k];
+        }
+      }
+    }
+    __threadfence();
+    __syncthreads();
+  }
+}

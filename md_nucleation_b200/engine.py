@@ -1,0 +1,204 @@
+"""Python binding of the engine's C ABI (include/mdn.h), loaded from the
+in-tree library md_nucleation_b200/lib/libmdn.so.
+
+The binding fails loudly when the library is missing or no CUDA device is
+present; there is no CPU fallback.  ``Engine`` drives a batch of replicas the
+way ``MD::run`` drives one (reference src/run.cpp:17-74): ``step`` is n calls
+of ``MD::verlet``, ``make_pair`` is ``MD::make_pair``, ``recenter`` the
+re-centring between relaxation and production, ``set_nvt`` the thermostat
+switches (``MD::setNVE``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import abi
+from .system import ReplicaSpec, StateArrays, descs
+
+_LIB = None
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libmdn.so")
+
+
+class MdnError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"mdn error {code}: {msg}")
+        self.code = code
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(
+                f"{LIB_PATH} is missing: build it with python -m md_nucleation_b200.build")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        L.mdn_abi_version.restype = C.c_int
+        L.mdn_last_error.restype = C.c_char_p
+        L.mdn_default_options.argtypes = [C.POINTER(abi.Options)]
+        L.mdn_device_count.argtypes = [C.POINTER(C.c_int)]
+        L.mdn_create.argtypes = [C.POINTER(abi.ReplicaDesc), C.c_int, C.POINTER(abi.Options), C.POINTER(vp)]
+        L.mdn_destroy.argtypes = [vp]
+        L.mdn_step.argtypes = [vp, C.c_longlong, C.c_int]
+        L.mdn_make_pair.argtypes = [vp]
+        L.mdn_recenter.argtypes = [vp, C.c_int]
+        L.mdn_set_nvt.argtypes = [vp, C.c_int, C.c_int, C.c_double]
+        L.mdn_compute_forces.argtypes = [vp, C.c_uint]
+        L.mdn_energies.argtypes = [vp, C.POINTER(C.c_double)]
+        L.mdn_get_status.argtypes = [vp, C.POINTER(C.c_int)]
+        L.mdn_clear_status.argtypes = [vp]
+        L.mdn_replica_info_get.argtypes = [vp, C.c_int, C.POINTER(abi.ReplicaInfo)]
+        L.mdn_download_state.argtypes = [vp, C.c_int, C.POINTER(abi.State)]
+        L.mdn_upload_state.argtypes = [vp, C.c_int, C.POINTER(abi.State)]
+        L.mdn_pair_list.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_int)]
+        L.mdn_in_domain.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                    C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.mdn_events.argtypes = [vp, C.POINTER(abi.Event), C.c_int, C.POINTER(C.c_int)]
+        L.mdn_kinetic.argtypes = [vp, C.POINTER(C.c_double)]
+        L.mdn_last_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
+        L.mdn_set_launch.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+        if L.mdn_abi_version() != abi.ABI_VERSION:
+            raise RuntimeError("libmdn.so ABI version mismatch")
+        _LIB = L
+    return _LIB
+
+
+def _ck(rc):
+    if rc != abi.OK:
+        raise MdnError(rc, lib().mdn_last_error().decode())
+
+
+def device_count() -> int:
+    n = C.c_int(0)
+    lib().mdn_device_count(C.byref(n))
+    return n.value
+
+
+def default_options(**kw) -> abi.Options:
+    o = abi.Options()
+    lib().mdn_default_options(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class Engine:
+    """A batch of replicas resident on one GPU."""
+
+    def __init__(self, specs: Sequence[ReplicaSpec], **options):
+        self.specs = list(specs)
+        self.L = lib()
+        self._descs, self._keep = descs(self.specs)
+        self.opt = default_options(**options)
+        h = C.c_void_p()
+        _ck(self.L.mdn_create(self._descs, len(self.specs), C.byref(self.opt), C.byref(h)))
+        self.h = h
+
+    @property
+    def n(self):
+        return len(self.specs)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.mdn_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- stepping -------------------------------------------------------------
+    def step(self, n: int = 1, energy_mode: int = 0):
+        _ck(self.L.mdn_step(self.h, n, energy_mode))
+
+    def make_pair(self):
+        _ck(self.L.mdn_make_pair(self.h))
+
+    def recenter(self, compat: bool = True):
+        _ck(self.L.mdn_recenter(self.h, 1 if compat else 0))
+
+    def set_nvt(self, mode: int, temperature: float = 300.0, replica: int = -1):
+        _ck(self.L.mdn_set_nvt(self.h, replica, mode, temperature))
+
+    def compute_forces(self, term_mask: int = 0):
+        _ck(self.L.mdn_compute_forces(self.h, term_mask))
+
+    def set_launch(self, cluster_size=0, threads=0, steps_per_launch=-1):
+        _ck(self.L.mdn_set_launch(self.h, cluster_size, threads, steps_per_launch))
+
+    # ---- results --------------------------------------------------------------
+    def energies(self) -> np.ndarray:
+        U = np.zeros((self.n, 8))
+        _ck(self.L.mdn_energies(self.h, abi.ptr(U)))
+        return U
+
+    def status(self) -> np.ndarray:
+        s = np.zeros(self.n, np.int32)
+        _ck(self.L.mdn_get_status(self.h, abi.ptr(s, C.c_int)))
+        return s
+
+    def clear_status(self):
+        _ck(self.L.mdn_clear_status(self.h))
+
+    def info(self, r: int = 0) -> abi.ReplicaInfo:
+        i = abi.ReplicaInfo()
+        _ck(self.L.mdn_replica_info_get(self.h, r, C.byref(i)))
+        return i
+
+    def state(self, r: int = 0) -> StateArrays:
+        s = StateArrays.for_spec(self.specs[r])
+        st = s.to_c()
+        _ck(self.L.mdn_download_state(self.h, r, C.byref(st)))
+        s.pull_scalars(st)
+        return s
+
+    def upload(self, r: int, s: StateArrays):
+        st = s.to_c()
+        _ck(self.L.mdn_upload_state(self.h, r, C.byref(st)))
+
+    def pair_list(self, r: int, kind: int) -> np.ndarray:
+        cnt = C.c_int(0)
+        _ck(self.L.mdn_pair_list(self.h, r, kind, None, 0, C.byref(cnt)))
+        buf = np.zeros((max(cnt.value, 1), 2), np.int32)
+        _ck(self.L.mdn_pair_list(self.h, r, kind, abi.ptr(buf, C.c_int), cnt.value, C.byref(cnt)))
+        return buf[:cnt.value]
+
+    def in_domain(self, r: int = 0):
+        cnt = C.c_int(0)
+        _ck(self.L.mdn_in_domain(self.h, r, 0, C.byref(cnt), None, None, None))
+        n = cnt.value
+        t = np.zeros(max(n, 1), np.int32)
+        x = np.zeros((max(n, 1), 3))
+        v = np.zeros((max(n, 1), 3))
+        _ck(self.L.mdn_in_domain(self.h, r, n, C.byref(cnt), abi.ptr(t, C.c_int), abi.ptr(x), abi.ptr(v)))
+        return t[:n], x[:n], v[:n]
+
+    def events(self):
+        cnt = C.c_int(0)
+        cap = 65536
+        buf = (abi.Event * cap)()
+        _ck(self.L.mdn_events(self.h, buf, cap, C.byref(cnt)))
+        return [buf[i] for i in range(min(cnt.value, cap))]
+
+    def kinetic(self) -> np.ndarray:
+        out = np.zeros((self.n, 4))
+        _ck(self.L.mdn_kinetic(self.h, abi.ptr(out)))
+        return out
+
+    def last_timing(self):
+        ms = C.c_double(0)
+        n = C.c_longlong(0)
+        _ck(self.L.mdn_last_timing(self.h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value

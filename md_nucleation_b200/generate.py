@@ -174,103 +174,156 @@ def nacl_cluster() -> Species:
 def chain(n_atoms: int, charge: float, rng: np.random.Generator) -> Species:
     """A +q peptide-like chain: a self-avoiding heavy-atom backbone (bonds
     1.33-1.53 A, angles 110-120 deg, torsions of periodicity 1-3 with barriers
-    0-2 kcal/mol) carrying two hydrogens per heavy atom at 1.0-1.09 A; charges
-    N(0, 0.3 e) shifted to the net charge; LJ sigma 2.5-3.5 A, eps 0.02-0.2."""
+    0-2 kcal/mol) carrying hydrogens at 1.0-1.09 A; charges N(0, 0.3 e) shifted
+    to the net charge; LJ sigma 2.5-3.5 A, eps 0.02-0.2.  Hydrogens are turned
+    about their heavy atom for the largest clearance, and a geometry is kept
+    only if every pair outside the AMBER exclusions (1-2, 1-3, 1-4) is at
+    least 0.8 sigma apart."""
     n_heavy = max(3, n_atoms // 3)
     n_h = n_atoms - n_heavy
     n_heavy_types = 6
-    # backbone, grown as a self-avoiding walk
-    for _attempt in range(200):
+    per = np.full(n_heavy, n_h // n_heavy)
+    per[: n_h % n_heavy] += 1
+    hpar = [i for i in range(n_heavy) for _ in range(per[i])]
+    mass = list(rng.choice([12.011, 14.007, 15.999], n_heavy_types)) + [1.008]
+    eps = list(rng.uniform(0.02, 0.2, n_heavy_types)) + [0.02]
+    sigma = list(rng.uniform(2.5, 3.5, n_heavy_types)) + [2.2]
+    types = list(rng.integers(0, n_heavy_types, n_heavy)) + [n_heavy_types] * n_h
+    sig = np.array([sigma[t] for t in types])
+    n = n_heavy + n_h
+    hs_of = [[] for _ in range(n_heavy)]
+    for h, p_ in enumerate(hpar):
+        hs_of[p_].append(n_heavy + h)
+    # topology (independent of the geometry)
+    bonds = [(i, i + 1) for i in range(n_heavy - 1)] + [(p_, n_heavy + h) for h, p_ in enumerate(hpar)]
+    angles = [(i - 1, i, i + 1) for i in range(1, n_heavy - 1)]
+    for i in range(n_heavy):
+        for hh in hs_of[i]:
+            for j in (i - 1, i + 1):
+                if 0 <= j < n_heavy:
+                    angles.append((hh, i, j))
+        for a in range(len(hs_of[i])):
+            for b in range(a + 1, len(hs_of[i])):
+                angles.append((hs_of[i][a], i, hs_of[i][b]))
+    dihed = [(i, i + 1, i + 2, i + 3) for i in range(n_heavy - 3)]
+    hdih = []
+    for i in range(n_heavy):
+        for hh in hs_of[i]:
+            if i + 2 < n_heavy:
+                hdih.append((hh, i, i + 1, i + 2))
+            if i - 2 >= 0:
+                hdih.append((hh, i, i - 1, i - 2))
+            if i + 1 < n_heavy:
+                for h2 in hs_of[i + 1]:
+                    hdih.append((hh, i, i + 1, h2))
+    excl = set()
+    for a, b in bonds:
+        excl.add((min(a, b), max(a, b)))
+    for a, _, c in angles:
+        excl.add((min(a, c), max(a, c)))
+    for a, _, _, d in dihed + hdih:
+        excl.add((min(a, d), max(a, d)))
+
+    def clearance_ok(xs):
+        d = np.linalg.norm(xs[:, None] - xs[None], axis=2)
+        lim = 0.8 * 0.5 * (sig[:, None] + sig[None, :])
+        bad = d < lim
+        for (a, b) in excl:
+            bad[a, b] = bad[b, a] = False
+        np.fill_diagonal(bad, False)
+        return not bad.any()
+
+    for _attempt in range(400):
         bb = [np.zeros(3)]
         bl = rng.uniform(1.33, 1.53, n_heavy)
         ok = True
         for i in range(1, n_heavy):
             for _try in range(200):
                 if i == 1:
-                    d = rng.normal(size=3); d /= np.linalg.norm(d)
+                    d = rng.normal(size=3)
+                    d /= np.linalg.norm(d)
                 else:
-                    prev = bb[-1] - bb[-2]; prev /= np.linalg.norm(prev)
+                    prev = bb[-1] - bb[-2]
+                    prev /= np.linalg.norm(prev)
                     th = rng.uniform(110, 120) * DEG
-                    perp = np.cross(prev, rng.normal(size=3)); perp /= np.linalg.norm(perp)
+                    perp = _perp(prev, rng)
                     d = math.cos(math.pi - th) * prev + math.sin(math.pi - th) * perp
                 cand = bb[-1] + bl[i] * d
-                if all(np.linalg.norm(cand - p) > 3.0 for p in bb[:-2]):
-                    bb.append(cand); break
+                if all(np.linalg.norm(cand - p_) > 3.6 for p_ in bb[:-2]):
+                    bb.append(cand)
+                    break
             else:
-                ok = False; break
-        if ok:
+                ok = False
+                break
+        if not ok:
+            continue
+        bb = np.array(bb)
+        xs = np.zeros((n, 3))
+        xs[:n_heavy] = bb
+        for i in range(n_heavy):
+            if not hs_of[i]:
+                continue
+            nb = [j for j in (i - 1, i + 1) if 0 <= j < n_heavy]
+            u = -sum((bb[j] - bb[i]) / np.linalg.norm(bb[j] - bb[i]) for j in nb)
+            if np.linalg.norm(u) < 1e-3:
+                u = _perp(bb[nb[0]] - bb[i], rng)
+            u /= np.linalg.norm(u)
+            w0 = _perp(u, rng)
+            best, best_pos = -1.0, None
+            for k in range(24):
+                phi = 2 * math.pi * k / 24
+                w = w0 * math.cos(phi) + np.cross(u, w0) * math.sin(phi)
+                pos = []
+                for hidx, hh in enumerate(hs_of[i]):
+                    ang = phi + 2 * math.pi * hidx / len(hs_of[i])
+                    v = w0 * math.cos(ang) + np.cross(u, w0) * math.sin(ang)
+                    dirn = math.cos(54.75 * DEG) * u + math.sin(54.75 * DEG) * v
+                    pos.append(bb[i] + 1.045 * dirn)
+                pos = np.array(pos)
+                others = np.concatenate([bb[[j for j in range(n_heavy) if abs(j - i) > 1]],
+                                         xs[n_heavy:][[h for h in range(n_h) if hpar[h] < i]]])
+                m = np.linalg.norm(pos[:, None] - others[None], axis=2).min() if len(others) else 9.0
+                if m > best:
+                    best, best_pos = m, pos
+            for hidx, hh in enumerate(hs_of[i]):
+                xs[hh] = best_pos[hidx]
+        for h in range(n_h):  # bond lengths 1.0-1.09 A
+            p_ = hpar[h]
+            dv = xs[n_heavy + h] - xs[p_]
+            xs[n_heavy + h] = xs[p_] + dv / np.linalg.norm(dv) * rng.uniform(1.0, 1.09)
+        if clearance_ok(xs):
             break
-    bb = np.array(bb)
-    # hydrogens: distributed over heavy atoms, placed off the backbone
-    per = np.full(n_heavy, n_h // n_heavy); per[: n_h % n_heavy] += 1
-    xs = list(bb)
-    types = list(rng.integers(0, n_heavy_types, n_heavy))
-    hpos, hpar = [], []
-    for i in range(n_heavy):
-        nb = [j for j in (i - 1, i + 1) if 0 <= j < n_heavy]
-        u = -sum((bb[j] - bb[i]) / np.linalg.norm(bb[j] - bb[i]) for j in nb)
-        if np.linalg.norm(u) < 1e-3:
-            u = _perp(bb[nb[0]] - bb[i], rng)
-        u /= np.linalg.norm(u)
-        w = _perp(u, rng)
-        for h in range(per[i]):
-            ang = 2 * math.pi * h / max(per[i], 1)
-            v = w * math.cos(ang) + np.cross(u, w) * math.sin(ang)
-            d = math.cos(54.75 * DEG) * u + math.sin(54.75 * DEG) * v
-            hpos.append(bb[i] + rng.uniform(1.0, 1.09) * d)
-            hpar.append(i)
-    xs = np.array(xs + hpos)
-    types = types + [n_heavy_types] * n_h
-    n = len(xs)
-    # bonded topology: one bond type / angle type / dihedral type per term,
-    # equilibrium values taken from the generated geometry
-    bonds, bond_coeff = [], []
-    def add_bond(i, j, K):
-        bonds.append([i, j, len(bond_coeff)])
+    else:
+        raise RuntimeError("could not grow a clash-free chain")
+    # bonded parameters: one type per term, equilibrium values from the geometry
+    bond_rows, bond_coeff = [], []
+    for (i, j) in bonds:
+        K = rng.uniform(250, 400) if j < n_heavy else 340.0
+        bond_rows.append([i, j, len(bond_coeff)])
         bond_coeff.append([K, float(np.linalg.norm(xs[i] - xs[j]))])
-    for i in range(n_heavy - 1):
-        add_bond(i, i + 1, rng.uniform(250, 400))
-    for h, p in enumerate(hpar):
-        add_bond(p, n_heavy + h, 340.0)
-    angles, angle_coeff = [], []
-    def add_angle(i, j, k, K):
-        angles.append([i, j, k, len(angle_coeff)])
+    angle_rows, angle_coeff = [], []
+    for (i, j, k) in angles:
+        K = rng.uniform(40, 70) if (i < n_heavy and k < n_heavy) else (35.0 if (i >= n_heavy and k >= n_heavy) else 50.0)
+        angle_rows.append([i, j, k, len(angle_coeff)])
         angle_coeff.append([K, _angle(xs[i], xs[j], xs[k])])
-    for i in range(1, n_heavy - 1):
-        add_angle(i - 1, i, i + 1, rng.uniform(40, 70))
-    hs_of = [[] for _ in range(n_heavy)]
-    for h, p in enumerate(hpar):
-        hs_of[p].append(n_heavy + h)
-    for i in range(n_heavy):
-        for hh in hs_of[i]:
-            for j in (i - 1, i + 1):
-                if 0 <= j < n_heavy:
-                    add_angle(hh, i, j, 50.0)
-        for a in range(len(hs_of[i])):
-            for b in range(a + 1, len(hs_of[i])):
-                add_angle(hs_of[i][a], i, hs_of[i][b], 35.0)
-    dihedrals, dih_multi, dih_coeff = [], [], []
-    for i in range(n_heavy - 3):
-        dihedrals.append([i, i + 1, i + 2, i + 3, len(dih_multi)])
+    dih_rows, dih_multi, dih_coeff = [], [], []
+    for t in dihed:
         nt = int(rng.integers(1, 3))
-        terms = [(rng.uniform(0, 2), int(rng.integers(1, 4)), float(rng.choice([0.0, 180.0])))
-                 for _ in range(nt)]
+        terms = [(rng.uniform(0, 2), int(rng.integers(1, 4)), float(rng.choice([0.0, 180.0]))) for _ in range(nt)]
+        dih_rows.append(list(t) + [len(dih_multi)])
         dih_multi.append(nt)
         dih_coeff.append(_dih_row(terms))
-    for i in range(n_heavy - 2):
-        for hh in hs_of[i]:
-            dihedrals.append([hh, i, i + 1, i + 2, len(dih_multi)])
-            dih_multi.append(1)
-            dih_coeff.append(_dih_row([(rng.uniform(0, 0.5), 3, 0.0)]))
+    for t in hdih:
+        dih_rows.append(list(t) + [len(dih_multi)])
+        dih_multi.append(1)
+        dih_coeff.append(_dih_row([(rng.uniform(0, 0.3), 3, 0.0)]))
     q = rng.normal(0, 0.3, n)
     q += (charge - q.sum()) / n
-    xs -= xs.mean(axis=0)
+    xs = xs - xs.mean(axis=0)
     return Species(
         names=[f"X{k}" for k in range(n_heavy_types)] + ["H"],
-        mass=list(rng.choice([12.011, 14.007, 15.999], n_heavy_types)) + [1.008],
-        eps=list(rng.uniform(0.02, 0.2, n_heavy_types)) + [0.02],
-        sigma=list(rng.uniform(2.5, 3.5, n_heavy_types)) + [2.5],
-        top=Topology(type=types, charge=q, x=xs, bonds=bonds, angles=angles, dihedrals=dihedrals),
+        mass=mass, eps=eps, sigma=sigma,
+        top=Topology(type=types, charge=q, x=xs, bonds=bond_rows, angles=angle_rows, dihedrals=dih_rows),
         bond_coeff=np.array(bond_coeff), angle_coeff=np.array(angle_coeff),
         dih_multi=np.array(dih_multi, np.int32), dih_coeff=np.array(dih_coeff),
         h_types=(n_heavy_types,))

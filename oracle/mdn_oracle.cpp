@@ -45,8 +45,10 @@
  * converge to the same constrained positions (the correction direction and
  * the stopping test (s^2 - d^2)^2 <= 1e-20 are the same); this file and the
  * engine use the textbook multiplier, sweep the constraints in colour order
- * (constraints of one colour share no atom) and stop after 1000 sweeps with
- * a status bit.  Unless MDN_Q_SHAKE_NO_VCORR is set, the half-step velocity
+ * (constraints of one colour share no atom), test convergence after a whole
+ * sweep (so the returned positions satisfy the tolerance, which the
+ * reference's per-constraint test does not guarantee) and stop after 1000
+ * sweeps with a status bit.  Unless MDN_Q_SHAKE_NO_VCORR is set, the half-step velocity
  * receives the constraint displacement divided by dt.
  */
 #include <algorithm>
@@ -230,14 +232,21 @@ struct Oracle {
       }
   }
 
-  /* SHAKE of one molecule: x = drifted positions, r = positions before drift */
+  /* SHAKE of one molecule: x = drifted positions, r = positions before drift.
+   * Sweeps in colour order; converged when every constraint satisfies
+   * (s^2 - d^2)^2 <= 1e-20 after a full sweep. */
   void shake_mol(const Top& t, V3* x, V3* v, const V3* r) {
     if (t.rigid.empty()) return;
     std::vector<V3> x0(x, x + t.n);
+    auto resid = [&](size_t k) {
+      int i = t.rigid[k][0], j = t.rigid[k][1];
+      double dk = bond_c[t.rigid[k][2]][1];
+      double sx = x[i][0] - x[j][0], sy = x[i][1] - x[j][1], sz = x[i][2] - x[j][2];
+      double dr = sx * sx + sy * sy + sz * sz - dk * dk;
+      return dr * dr;
+    };
     bool converge = false;
-    int sweeps = 0;
-    while (!converge) {
-      converge = true;
+    for (int sweep = 0; sweep < 1000 && !converge; sweep++) {
       for (int c = 0; c < t.n_colors; c++)
         for (size_t k = 0; k < t.rigid.size(); k++) {
           if (t.rigid_color[k] != c) continue;
@@ -253,16 +262,12 @@ struct Oracle {
           double ci = g / t.mass[i], cj = g / t.mass[j];
           x[i][0] += rx * ci; x[i][1] += ry * ci; x[i][2] += rz * ci;
           x[j][0] -= rx * cj; x[j][1] -= ry * cj; x[j][2] -= rz * cj;
-          sx = x[i][0] - x[j][0]; sy = x[i][1] - x[j][1]; sz = x[i][2] - x[j][2];
-          s2 = sx * sx + sy * sy + sz * sz;
-          double dr = s2 - dk * dk;
-          if (dr * dr > 1e-20) converge = false;
         }
-      if (++sweeps >= 1000 && !converge) {
-        status |= MDN_ST_SHAKE_NOCONV;
-        break;
-      }
+      converge = true;
+      for (size_t k = 0; k < t.rigid.size(); k++)
+        if (resid(k) > 1e-20) converge = false;
     }
+    if (!converge) status |= MDN_ST_SHAKE_NOCONV;
     if (!(quirks & MDN_Q_SHAKE_NO_VCORR))
       for (int a = 0; a < t.n; a++)
         for (int k = 0; k < 3; k++) v[a][k] += (x[a][k] - x0[a][k]) / dt;
@@ -420,6 +425,12 @@ struct Oracle {
     V3* v = &vv[(size_t)m * a_v];
     V3* f = &vf[(size_t)m * a_v];
     for (int a = 0; a < a_v; a++) { x[a] = vap.x[a]; v[a] = {0, 0, 0}; f[a] = {0, 0, 0}; }
+    /* MD::update_position ran before this rebuild, while the molecule was
+     * outside, so its weights are not set for the current step: a first entry
+     * has 0 (initializationVapor.cpp:70-71); a re-entry would carry the weights
+     * of its previous visit, which this restatement (and the engine) also
+     * sets to 0 */
+    for (int a = 0; a < a_v; a++) vw[(size_t)m * a_v + a] = 0;
     orc::U4 s = draw(mi, 1, 0);
     double a = orc::u01(s.v[0]) * 2 * M_PI;
     double b = orc::u01(s.v[1]) * 2 * M_PI;

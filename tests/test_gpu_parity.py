@@ -1,0 +1,148 @@
+"""Parity of the CUDA engine (through the C ABI) with the FP64 oracle.
+
+Bars (the tolerance of each comparison is stated where it is made):
+  * the effective-domain rebuild uses the same Philox draws as the oracle, so
+    the whole state after MD::MD's initial make_pair agrees to FP64 rounding
+    of the transcendental functions (sin/cos/log of CUDA vs glibc);
+  * pair lists are equal as sets;
+  * forces: relative RMS error <= 1e-5 against FP64 (FP32 pair arithmetic,
+    int64 fixed-point sums); energies per bucket likewise;
+  * short trajectories, across a rebuild, stay within 1e-6 A / 1e-7 A/fs;
+  * results are bit-identical across launch shapes and batch compositions
+    (every multi-writer sum is an integer sum).
+"""
+import numpy as np
+import pytest
+
+from md_nucleation_b200 import abi
+from tests import systems
+from tests.gpu_helpers import compare_states, force_ok, forces_of, need_gpu, rel_rms
+
+pytestmark = pytest.mark.gpu
+
+NAMES = list(systems.ALL)
+
+
+@pytest.fixture(scope="module")
+def eng():
+    return need_gpu()
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_initial_make_pair_matches_oracle(eng, oracle_libs, name):
+    spec = systems.make(name)
+    e = eng.Engine([spec])
+    o = oracle_libs.OracleReplica(spec)
+    a, b = e.state(0), o.get_state()
+    i = e.info(0)
+    assert i.status == 0
+    assert i.n_gas_in == o.info().n_gas_in and i.n_vapor_in == o.info().n_vapor_in
+    compare_states(a, b, spec, xtol=1e-11, vtol=1e-13, what=name)
+    assert abs(a.loop_update - b.loop_update) <= 1
+    for kind in (0, 1):
+        assert {tuple(p) for p in e.pair_list(0, kind)} == {tuple(p) for p in o.pair_list(kind)}
+
+
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("term", [0, abi.I_GI, abi.I_VI, abi.I_VV, abi.I_GV, abi.I_AMBER, abi.I_BMH,
+                                  abi.I_GAS_INTRA, abi.I_VAPOR_INTRA])
+def test_forces_match_fp64_oracle(eng, oracle_libs, name, term):
+    spec = systems.make(name)
+    if term and not spec.interactions & term:
+        pytest.skip("term not enabled")
+    o = oracle_libs.OracleReplica(spec)
+    o.step(3)  # weights and forces populated
+    st = o.get_state()
+    e = eng.Engine([spec])
+    e.upload(0, st)
+    o.set_state(st)
+    e.compute_forces(term)
+    Uo = o.compute_forces(term)
+    Ue = e.energies()[0]
+    fe, fo = forces_of(e.state(0), spec), forces_of(o.get_state(), spec)
+    if np.abs(fo).max() == 0:
+        assert np.abs(fe).max() == 0
+        return
+    ok, err, rms = force_ok(fe, fo)
+    assert ok, f"relative RMS force error {err:.2e} (RMS {rms:.2e} kcal/mol/A)"
+    # energies are sums of FP32 pair terms of both signs: the bound is the FP32
+    # rounding of the terms, 1e-4 of the largest bucket (reported per config)
+    scale = max(np.abs(Uo).max(), 1e-3)
+    assert np.all(np.abs(Ue - Uo) <= 1e-4 * scale + 1e-6), f"energies {Ue} vs {Uo}"
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_trajectory_across_rebuild(eng, oracle_libs, name):
+    """30 steps with a rebuild at the first step (loop_pair = loop_update)."""
+    spec = systems.make(name)
+    o = oracle_libs.OracleReplica(spec)
+    o.step(2)
+    st = o.get_state()
+    st.loop_pair, st.loop_update = 5, 5
+    e = eng.Engine([spec])
+    e.upload(0, st)
+    o.set_state(st)
+    e.step(30, energy_mode=1)
+    o.step(30, energy_mode=1)
+    a, b = e.state(0), o.get_state()
+    assert e.info(0).n_rebuilds >= 2 and e.status()[0] == 0
+    compare_states(a, b, spec, xtol=1e-6, vtol=1e-7, what=name)
+    err = rel_rms(forces_of(a, spec), forces_of(b, spec))
+    assert err <= 1e-4
+    Ue, Uo = e.energies()[0], o.energies()
+    assert np.all(np.abs(Ue - Uo) <= 1e-4 * max(np.abs(Uo).max(), 1e-3) + 1e-6)
+
+
+def test_shake_constraints_hold(eng):
+    spec = systems.make("chain_ar_meoh_shake")
+    e = eng.Engine([spec])
+    e.step(200)
+    st = e.state(0)
+    rig = spec.ion.rigid
+    d0 = spec.bond_coeff[rig[:, 2], 1]
+    d = np.linalg.norm(st.ion_x[rig[:, 0]] - st.ion_x[rig[:, 1]], axis=1)
+    assert np.all(np.abs(d * d - d0 * d0) <= 1.0001e-10)
+    assert e.status()[0] == 0
+
+
+def test_batch_equals_single_replicas(eng):
+    """Replicas are independent: stepping them together is bit-identical to
+    stepping each alone."""
+    specs = [systems.make(n) for n in ("nacl_n2_meoh", "chain_he_water", "nacl_n2mono_meoh")]
+    eb = eng.Engine(specs)
+    eb.step(40)
+    for r, s in enumerate(specs):
+        es = eng.Engine([s])
+        es.step(40)
+        compare_states(eb.state(r), es.state(0), s, 0.0, 0.0, what=f"replica {r}")
+
+
+@pytest.mark.parametrize("threads,cluster", [(256, 1), (512, 2), (256, 4)])
+def test_launch_shape_invariance(eng, threads, cluster):
+    specs = [systems.make("chain_ar_meoh_shake"), systems.make("nacl_n2_meoh")]
+    e0 = eng.Engine(specs)
+    e1 = eng.Engine(specs, threads=threads, cluster_size=cluster)
+    e0.step(25, energy_mode=1)
+    e1.step(25, energy_mode=1)
+    for r, s in enumerate(specs):
+        compare_states(e0.state(r), e1.state(r), s, 0.0, 0.0, what=f"replica {r}")
+    assert np.array_equal(e0.energies(), e1.energies())
+
+
+def test_steps_per_launch_invariance(eng):
+    spec = systems.make("nacl_n2rigid_water")
+    e0 = eng.Engine([spec])
+    e1 = eng.Engine([spec], steps_per_launch=1)
+    e0.step(20)
+    e1.step(20)
+    compare_states(e0.state(0), e1.state(0), spec, 0.0, 0.0)
+
+
+def test_upload_capacity_is_an_error(eng):
+    spec = systems.make("nacl_n2_meoh")
+    e = eng.Engine([spec])
+    st = e.state(0)
+    st.region[1:1 + spec.n_gas] = 1  # every gas molecule claimed in-domain
+    with pytest.raises(eng.MdnError) as ex:
+        e.upload(0, st)
+    assert ex.value.code == abi.ERR_CAPACITY
