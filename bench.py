@@ -1,0 +1,433 @@
+"""Throughput of the batched replica workload: 256 independent nucleation
+replicas (gas He/Ar/N2/N2-monoatomic, 5,000-100,000 molecules; methanol or
+3-site water vapor, 10-300 molecules; NaCl cluster or a 50-300 atom +1 chain;
+500-20,000 atoms inside each 10 nm effective domain; SHAKE on X-H bonds;
+300 K, dt = 1 fs), advanced 100 MD steps per bench step by the persistent
+step kernel.
+
+metric: in-domain atom-steps per second, summed over replicas (the atoms the
+reference's pair forces and dump loop visit, src/output/output.cpp:136-143).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--replicas R]
+  python bench.py --impl reference ...   the reference's own CPU routines
+                                         (oracle/_ref) on the host cores
+
+Under torchrun every rank runs its own R replicas (seeds offset by rank):
+weak scaling, no data-path collective.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "replica atom-steps/s on 1 B200, batched vs plain at force err≤1e-5; adjoint/fwd"
+UNIT = "atom-steps/s"
+MD_STEPS = 100          # MD steps per bench step (one bench step = one 100-step block)
+WORKLOAD = "batched replicas: 256 independent systems, 100 MD steps per step"
+
+# FP32 flops of one pair evaluation (distance, r^-2, r^-6, the LJ force
+# factor; + r^-1 and the Coulomb factor; BMH: + sqrt, exp and its r^-8 and
+# r^-10 terms): the algorithmic count takes each pair once.
+FLOPS_LJ = 20
+FLOPS_LJ_COUL = 29
+FLOPS_BMH = 35
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def _make_replica(r):
+    from md_nucleation_b200 import generate
+    return generate.config2_replica(r)
+
+
+def make_specs(first: int, n: int, workers: int):
+    """Generates the replicas in a spawn pool (the chain growth and the
+    placement of up to 100,000 molecules take seconds per replica)."""
+    t0 = time.time()
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(max(1, workers)) as pool:
+        specs = pool.map(_make_replica, range(first, first + n), chunksize=1)
+    log(f"generated {n} replicas in {time.time() - t0:.1f} s on {workers} workers")
+    return specs
+
+
+def in_domain_atoms(infos, specs):
+    return np.array([i.n_ion + i.n_gas_in * s.gas.n + i.n_vapor_in * s.vapor.n for i, s in zip(infos, specs)],
+                    np.int64)
+
+
+def algorithmic_flops(infos, specs):
+    """FP32 flops of one MD step's pair terms, each pair once:
+    gas-ion (gas atom x ion atom of listed molecule pairs, LJ), gas-vapor
+    (atoms of listed molecule pairs, LJ), vapor-ion and vapor-vapor (all
+    in-domain atoms, LJ + Coulomb), the ion's own non-bonded pairs (LJ +
+    Coulomb for a chain, BMH for a salt cluster)."""
+    from md_nucleation_b200 import abi
+    tot = 0.0
+    for i, s in zip(infos, specs):
+        ag, av, ni = s.gas.n, s.vapor.n, i.n_ion
+        vin = i.n_vapor_in * av
+        f = i.gi_pairs * ag * FLOPS_LJ + i.gv_pairs * ag * av * FLOPS_LJ
+        f += vin * ni * FLOPS_LJ_COUL
+        f += i.n_vapor_in * (i.n_vapor_in - 1) / 2 * av * av * FLOPS_LJ_COUL
+        ion_pairs = ni * (ni - 1) / 2
+        f += ion_pairs * (FLOPS_BMH if s.interactions & abi.I_BMH else FLOPS_LJ_COUL)
+        tot += f
+    return tot
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                out, _ = self.p.communicate(timeout=10)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+                out, _ = self.p.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, smax, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = max(smax, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def dist_init(ws, local, backend):
+    if ws == 1:
+        return None
+    import datetime
+    import torch
+    import torch.distributed as dist
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return dist
+
+
+def max_over_ranks(dist, value: float, device):
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(dist, value: float, device):
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's own routines, one replica per OpenMP thread
+# ---------------------------------------------------------------------------
+class stdout_to_stderr:
+    """Sends file descriptor 1 to stderr: the reference's constructor prints
+    its interaction table on stdout, which carries only the JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
+def cpu_sample(specs, threads: int, budget_s: float):
+    """Times the reference's MD::verlet (SHAKE step where the replica has
+    SHAKE) on `2 * threads` replicas spread over the batch, one replica per
+    OpenMP thread at a time (src/main.cpp:22-29); returns (atom-steps/s, what
+    was sampled).  The step count is sized from a 5-step calibration so the
+    sample takes about `budget_s`."""
+    from oracle import bind
+    stride = max(1, len(specs) // (2 * threads))
+    pick = list(range(0, len(specs), stride))[:2 * threads]
+    with stdout_to_stderr():
+        reps = [bind.RefReplica(specs[r]) for r in pick]
+    atoms = sum(r.in_domain_atoms() for r in reps)
+    t0 = time.perf_counter()
+    bind.ref_verlet_many(reps, 5, threads)
+    cal = (time.perf_counter() - t0) / 5
+    n = max(5, int(budget_s / max(cal, 1e-6)))
+    atoms0 = sum(r.in_domain_atoms() for r in reps)
+    t0 = time.perf_counter()
+    bind.ref_verlet_many(reps, n, threads)
+    dt = time.perf_counter() - t0
+    atoms1 = sum(r.in_domain_atoms() for r in reps)
+    value = 0.5 * (atoms0 + atoms1) * n / dt
+    sample = (f"{len(reps)} of the {len(specs)} replicas (every {stride}th), {n} MD steps each, "
+              f"{atoms} in-domain atoms at the start, {dt:.1f} s wall")
+    return value, sample, len(reps), n, dt
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    from oracle import bind
+    if not bind.have_reference():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_harness.so was not built"}))
+        return 0
+    threads = host_threads()
+    specs = make_specs(0, args.replicas, threads)
+    values = []
+    sample = ""
+    for k in range(args.warmup + args.steps):
+        v, sample, nrep, n, dt = cpu_sample(specs, threads, args.ref_budget)
+        if k >= args.warmup:
+            values.append(v)
+        log(f"reference step {k}: {v:.4g} atom-steps/s ({sample})")
+    value = float(np.mean(values))
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "replicas": args.replicas, "md_steps_per_step": MD_STEPS,
+                   "path": "reference routines (MD::verlet, SHAKE step where set) compiled from the "
+                           "reference sources, one replica per OpenMP thread"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# the CUDA engine
+# ---------------------------------------------------------------------------
+def run_engine(args):
+    ws, rank, local = dist_env()
+    threads = host_threads()
+    # replicas are generated in a spawn pool before any CUDA call
+    specs = make_specs(rank * args.replicas, args.replicas, max(1, threads // max(ws, 1)))
+    dist = dist_init(ws, local, "nccl")
+    import torch
+    from md_nucleation_b200 import abi, engine
+    if engine.device_count() == 0:
+        raise SystemExit("bench.py: no CUDA device")
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    free0, total = torch.cuda.mem_get_info(device)
+    checked = abi.Q_ALL & ~abi.Q_BLIND_INSERT
+    t0 = time.time()
+    eng = engine.Engine(specs, quirks=checked, device=local, use_graph=1)
+    free1, _ = torch.cuda.mem_get_info(device)
+    resident = free0 - free1
+    log(f"rank {rank}: engine created in {time.time() - t0:.1f} s, {resident / 2**30:.2f} GiB resident")
+
+    def barrier():
+        torch.cuda.synchronize(device)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(device)
+
+    for _ in range(args.warmup):
+        eng.step(MD_STEPS)
+    barrier()
+    infos0 = [eng.info(r) for r in range(eng.n)]
+    atoms0 = in_domain_atoms(infos0, specs)
+    flops0 = algorithmic_flops(infos0, specs)
+    # timed region: K bench steps, device time from CUDA events on the
+    # launching stream (mdn_last_timing)
+    ms_total, launches = 0.0, 0
+    barrier()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            eng.step(MD_STEPS)
+            ms, nl = eng.last_timing()
+            ms_total += ms
+            launches += nl
+        barrier()
+    infos1 = [eng.info(r) for r in range(eng.n)]
+    atoms1 = in_domain_atoms(infos1, specs)
+    flops1 = algorithmic_flops(infos1, specs)
+    status = eng.status()
+    fatal = int(np.sum((status & abi.ST_FATAL) != 0))
+    warned = int(np.sum((status != 0) & ((status & abi.ST_FATAL) == 0)))
+    atom_steps = 0.5 * float(atoms0.sum() + atoms1.sum()) * MD_STEPS * args.steps
+    ms_max = max_over_ranks(dist, ms_total, device)
+    atom_steps_all = sum_over_ranks(dist, atom_steps, device)
+    value = atom_steps_all / (ms_max * 1e-3)
+    flops_per_md_step = 0.5 * (flops0 + flops1)
+    achieved_tflops = flops_per_md_step * MD_STEPS * args.steps / (ms_total * 1e-3) / 1e12
+    clocks = clk.summary()
+
+    # end to end through the C ABI: per bench step the thermostat controls go
+    # host -> device from page-locked memory and every replica's in-domain
+    # atoms come back into page-locked host buffers (the dump path)
+    modes = engine.PinnedArray((eng.n,), np.int32)
+    temps = engine.PinnedArray((eng.n,), np.float64)
+    modes.array[:] = [s.nvt_mode for s in specs]
+    temps.array[:] = [s.nvt_temperature for s in specs]
+    cap = int(atoms1.max() * 1.5 * eng.n) + 1024
+    snap = engine.SnapshotBuffer(eng.n, cap, pinned=True)
+    e2e_steps = max(1, min(args.steps, 3))
+    barrier()
+    t0 = time.perf_counter()
+    d2h = 0
+    e2e_atom_steps = 0.0
+    for _ in range(e2e_steps):
+        eng.set_nvt_batch(modes.array, temps.array)
+        eng.step(MD_STEPS, energy_mode=1)
+        eng.snapshot(snap, energies=True)
+        d2h += snap.nbytes_used + (eng.n + 1) * 8 + eng.n * 64
+        e2e_atom_steps += float(snap.offset[-1]) * MD_STEPS
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(dist, e2e_s, device)
+    e2e_all = sum_over_ranks(dist, e2e_atom_steps, device)
+    e2e_value = e2e_all / e2e_s
+    h2d_per_step = eng.n * (4 + 8)
+
+    out = None
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 forces / f64 integration",
+            "data": "synthetic (seeded generator of the batched-replica configuration)",
+            "config": {
+                "workload": WORKLOAD, "replicas_per_gpu": eng.n, "md_steps_per_step": MD_STEPS,
+                "in_domain_atoms_per_gpu": int(atoms1.sum()),
+                "in_domain_atoms_range": [int(atoms1.min()), int(atoms1.max())],
+                "insertion": "checked (rotation re-drawn until no atom within 2 A)",
+                "l2": f"inputs larger than L2: {resident / 2**30:.2f} GiB resident per GPU",
+                "replicas_with_warnings": warned, "replicas_failed": fatal,
+                "parallelism": f"replicas sharded over {ws} GPU(s), no collective in the step",
+            },
+            "roofline": {
+                "bound": "fp32", "achieved": achieved_tflops,
+                "peak": None, "unit": "TFLOP/s", "frac": None, "traffic": None,
+                "kernel": "mdn_advance",
+                "algorithmic_flops_per_md_step": flops_per_md_step,
+            },
+            "gpu_launches": launches,
+            "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d_per_step,
+                    "d2h_bytes_per_step": int(d2h / e2e_steps)},
+        }
+        # FP32 peak: 148 SMs x 128 FP32 lanes x 2 flops (FMA) at the SM clock
+        # measured during the timed region (no FP32 figure is measured
+        # separately on these GPUs)
+        props = torch.cuda.get_device_properties(device)
+        mhz = clocks["sm_mhz"] or 1965.0
+        peak = props.multi_processor_count * 128 * 2 * mhz * 1e6 / 1e12
+        out["roofline"]["peak"] = peak
+        out["roofline"]["frac"] = achieved_tflops / peak
+        out["roofline"]["peak_source"] = (f"{props.multi_processor_count} SMs x 128 FP32 lanes x 2 "
+                                          f"at the measured {mhz:.0f} MHz")
+    # CPU baseline on rank 0 at N = 1 only
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        from oracle import bind
+        if bind.have_reference():
+            v, sample, nrep, n, dt = cpu_sample(specs, threads, args.cpu_budget)
+            out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+                                   "sample": sample}
+        else:
+            out["cpu_baseline"] = None
+    if rank == 0:
+        print(json.dumps(out))
+    eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--replicas", type=int, default=256)
+    ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of the CPU-baseline sample")
+    ap.add_argument("--ref-budget", type=float, default=10.0, help="seconds per reference-arm step")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and not os.environ.get("MDN_BENCH_ALLOW_SHORT"):
+        raise SystemExit("bench.py: --warmup must be >= 3")
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_engine(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

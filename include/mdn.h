@@ -23,6 +23,8 @@
 #ifndef MDN_H
 #define MDN_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -45,6 +47,13 @@ extern "C" {
 #define MDN_ST_NONFINITE       0x0010 /* a non-finite force, position or velocity */
 #define MDN_ST_FIXED_OVERFLOW  0x0020 /* a force left the 64-bit fixed-point range */
 #define MDN_ST_EVENT_OVERFLOW  0x0040 /* vapor in/out event log full (events dropped) */
+/* Fatal bits freeze the replica (later steps skip it) and make mdn_step
+ * return MDN_ERR_REPLICA; the others are warnings the replica runs on with:
+ * a molecule entering the domain is placed without an overlap test
+ * (src/pairList/updateGasIn.cpp:51-98), as in the reference, so an entry on
+ * top of another atom produces a huge force -- the reference carries on with
+ * it, the engine carries on with each pair term saturated at 2^21 kcal/mol/A. */
+#define MDN_ST_FATAL (MDN_ST_SLAB_OVERFLOW | MDN_ST_CORE_OVERFLOW | MDN_ST_LIST_OVERFLOW | MDN_ST_NONFINITE)
 
 /* ---- Interactions keywords (src/initialization/setCondition.cpp:186-228) - */
 #define MDN_I_GI           0x0001 /* gi LJ                     (PotentialGasIon)     */
@@ -73,9 +82,22 @@ extern "C" {
                                      -> Uion (src/potential/compute_intra.cpp:82,124,194) */
 #define MDN_Q_SHAKE_NO_VCORR 0x10 /* SHAKE moves positions only, no velocity
                                      correction (src/shake.cpp:6-92)          */
-#define MDN_Q_ALL            0x0F /* MDN_Q_SHAKE_NO_VCORR is opt-in: the reference never
+#define MDN_Q_BLIND_INSERT   0x20 /* a molecule entering the domain is placed with one
+                                     random rotation and no overlap test
+                                     (src/pairList/updateGasIn.cpp:51-98,
+                                     updateVaporIn.cpp:55-82).  Cleared: the rotation is
+                                     re-drawn (up to 4 draws) until no atom lies within
+                                     2 A of an ion or in-domain vapor atom (and, for an
+                                     entering vapor molecule, of an in-domain gas atom),
+                                     else the entry waits for the next rebuild.  At the
+                                     gas densities of 20,000 in-domain atoms the blind
+                                     form places atoms <0.5 A apart every few hundred
+                                     steps. */
+#define MDN_Q_ALL            0x2F /* MDN_Q_SHAKE_NO_VCORR is opt-in: the reference never
                                      calls its SHAKE (src/verlet.cpp:24), and the
                                      position-only form heats the system */
+#define MDN_INSERT_MIN_DIST 2.0  /* A, the overlap test of the checked insertion */
+#define MDN_INSERT_TRIES    4
 
 /* energy buckets, the order of `struct Potentials` (src/struct.hpp:29-38) */
 #define MDN_U_ION 0
@@ -229,6 +251,9 @@ int  mdn_make_pair(mdn_handle* h);
 int  mdn_recenter(mdn_handle* h, int compat);
 /* Thermostat of one replica (replica < 0: all); MDN_NVT_OFF is MD::setNVE. */
 int  mdn_set_nvt(mdn_handle* h, int replica, int mode, double temperature);
+/* Thermostat modes and targets of every replica from host arrays
+ * ([n_replicas] each; page-locked buffers make the copy asynchronous). */
+int  mdn_set_nvt_batch(mdn_handle* h, const int* mode, const double* temperature);
 /* Recomputes forces (and energies) on the current positions without moving
  * anything; term_mask selects MDN_I_* terms (0 = all enabled terms).      */
 int  mdn_compute_forces(mdn_handle* h, unsigned int term_mask);
@@ -248,6 +273,21 @@ int  mdn_pair_list(mdn_handle* h, int replica, int kind, int* pairs, int capacit
  * src/output/output.cpp:133-170), molecule order, ion first.            */
 int  mdn_in_domain(mdn_handle* h, int replica, int capacity, int* count,
                    int* type, double* x, double* v);
+/* Every replica's in-domain atoms plus the energies of the last mdn_step, in
+ * one batched copy (device-side compaction, then one copy per array): the
+ * feed of the OVITO dump and the energy logs of MD::display
+ * (src/output/output.cpp:68-170) for the whole batch.  offset[r]..offset[r+1]
+ * are the rows of replica r (ion atoms, then gas atoms of in-domain molecules
+ * in ascending molecule order, then vapor atoms); type/x/v hold `capacity`
+ * rows (x, v: 3 doubles per row); U: [8*n_replicas] or NULL.  Host buffers
+ * from mdn_host_alloc make the copies asynchronous.  Returns
+ * MDN_ERR_CAPACITY, with offset filled, when capacity is too small.        */
+int  mdn_snapshot(mdn_handle* h, long long* offset, long long capacity, int* type, double* x, double* v,
+                  double* U);
+/* Page-locked host memory for mdn_snapshot / mdn_upload_state buffers. */
+int  mdn_host_alloc(size_t bytes, void** ptr);
+int  mdn_host_free(void* ptr);
+
 /* Drains the vapor in/out event log of every replica. */
 int  mdn_events(mdn_handle* h, mdn_event* ev, int capacity, int* count);
 /* Kinetic energies (MD Observer::computeProps, src/output/observer.cpp:5-36):
@@ -259,6 +299,11 @@ int  mdn_kinetic(mdn_handle* h, double* out);
  * stream the kernels were launched on; kernel_launches = kernels issued.  */
 int  mdn_last_timing(mdn_handle* h, double* ms, long long* kernel_launches);
 int  mdn_set_launch(mdn_handle* h, int cluster_size, int threads, int steps_per_launch);
+/* Per-replica SM-cycle accounting of the step kernel: enable = 1 starts
+ * accumulating (from zero), 0 stops.  out: [8*n_replicas] cycles per phase:
+ * total, core integration, gas integration, rebuild, near gas molecules,
+ * core bonded terms, core pair terms, core force sums and kick. */
+int  mdn_profile(mdn_handle* h, int enable, long long* out);
 
 #ifdef __cplusplus
 }

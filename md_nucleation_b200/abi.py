@@ -16,6 +16,7 @@ ST_SHAKE_NOCONV = 0x0008
 ST_NONFINITE = 0x0010
 ST_FIXED_OVERFLOW = 0x0020
 ST_EVENT_OVERFLOW = 0x0040
+ST_FATAL = ST_SLAB_OVERFLOW | ST_CORE_OVERFLOW | ST_LIST_OVERFLOW | ST_NONFINITE
 
 I_GI = 0x0001
 I_VI = 0x0002
@@ -34,7 +35,10 @@ Q_GAS_ROT_ZY = 0x02
 Q_N2_ROT_VYVZ = 0x04
 Q_ENERGY_BUCKETS = 0x08
 Q_SHAKE_NO_VCORR = 0x10
-Q_ALL = 0x0F  # Q_SHAKE_NO_VCORR is opt-in
+Q_BLIND_INSERT = 0x20
+Q_ALL = 0x2F  # Q_SHAKE_NO_VCORR is opt-in
+INSERT_MIN_DIST = 2.0
+INSERT_TRIES = 4
 
 U_ION, U_GAS, U_VAP, U_GI, U_GG, U_VG, U_VI, U_VV = range(8)
 ENERGY_NAMES = ("Uion", "Ugas", "Uvap", "Ugi", "Ugg", "Uvg", "Uvi", "Uvv")

@@ -53,7 +53,6 @@ struct Core {
   double* v;        /* [3*nc] velocities                       */
   double* f;        /* [3*nc] force of the last evaluation     */
   long long* acc;   /* [2][3*nc] fixed-point partial sums      */
-  double* xold;     /* [3*nc] positions before the drift       */
   float4* pos;      /* [nc] (x - ion centre, charge), FP32     */
   float* w;         /* [nc] taper weight                       */
   int* type;        /* [nc] atom type                          */
@@ -75,6 +74,8 @@ struct Ctx {
   int n_core;       /* atoms in the core                */
   int buf;          /* which acc buffer holds this step */
   int* iscr;        /* >= 64 ints of scratch            */
+  int* cand;        /* [65] entering vapor molecules    */
+  double* trial;    /* [3*MDN_MAX_VAP_ATOMS] trial atoms */
   double* dscr;     /* >= 64 doubles of scratch         */
   const int* ib;    /* int blob of the replica          */
   const double* db; /* double blob of the replica       */
@@ -91,6 +92,17 @@ __device__ __forceinline__ size_t vatom(const RepParams* P, int parity, int s, i
 }
 __device__ __forceinline__ size_t vmol(const RepParams* P, int parity, int s) {
   return (size_t)P->vslab_moff + (size_t)parity * P->vcap + s;
+}
+
+/* per-phase SM cycles of the current job (thread 0 times phases that end in a
+ * block barrier); flushed to KArgs::prof at the end of the job */
+__shared__ long long s_prof[MDN_PROF_N];
+__shared__ long long s_prof_t0;
+__device__ __forceinline__ void prof_start(const Ctx& x) {
+  if (x.a->prof && threadIdx.x == 0) s_prof_t0 = clock64();
+}
+__device__ __forceinline__ void prof_end(const Ctx& x, int phase) {
+  if (x.a->prof && threadIdx.x == 0) s_prof[phase] += clock64() - s_prof_t0;
 }
 
 __device__ __forceinline__ void set_status(const Ctx& x, int bit) {
@@ -246,13 +258,17 @@ __device__ int shake_small(const Ctx& x, double* X, double* V, const double* R, 
 
 __device__ void core_drift_shake(Ctx& x) {
   const RepParams* P = x.P;
+  /* positions before the drift (the SHAKE reference vectors) live in the
+   * accumulation buffer this step's forces will use: it is zeroed only after
+   * SHAKE, and no CTA of the cluster reads it any more (see core_reduce) */
+  double* const xold = (double*)(x.c.acc + (size_t)x.buf * 3 * x.a->nc_cap);
   const bool sh = (P->interactions & MDN_I_SHAKE) != 0;
   const bool vcorr = !(P->quirks & MDN_Q_SHAKE_NO_VCORR);
   const double dt = P->dt;
   for (int i = threadIdx.x; i < x.n_core; i += blockDim.x) {
     for (int k = 0; k < 3; k++) {
       double xo = x.c.x[3 * i + k];
-      x.c.xold[3 * i + k] = xo;
+      xold[3 * i + k] = xo;
       x.c.x[3 * i + k] = xo + x.c.v[3 * i + k] * dt;
     }
   }
@@ -269,7 +285,7 @@ __device__ void core_drift_shake(Ctx& x) {
         for (int k = threadIdx.x; k < P->n_ion_rigid; k += blockDim.x) {
           if (col[k] != c) continue;
           int i = rig[3 * k], j = rig[3 * k + 1];
-          shake_pair(x.c.x, x.c.xold, i, j, x.db[P->d_bond + 2 * rig[3 * k + 2] + 1],
+          shake_pair(x.c.x, xold, i, j, x.db[P->d_bond + 2 * rig[3 * k + 2] + 1],
                      x.db[P->d_mass + x.c.type[i]], x.db[P->d_mass + x.c.type[j]]);
         }
         __syncthreads();
@@ -292,7 +308,7 @@ __device__ void core_drift_shake(Ctx& x) {
       for (int i = threadIdx.x; i < P->n_ion; i += blockDim.x)
         for (int k = 0; k < 3; k++) {
           /* displacement by the constraints = x - (xold + v*dt) */
-          double xd = x.c.xold[3 * i + k] + x.c.v[3 * i + k] * dt;
+          double xd = xold[3 * i + k] + x.c.v[3 * i + k] * dt;
           x.c.v[3 * i + k] += (x.c.x[3 * i + k] - xd) / dt;
         }
     __syncthreads();
@@ -309,7 +325,7 @@ __device__ void core_drift_shake(Ctx& x) {
         for (int k = 0; k < 3; k++) {
           X[3 * at + k] = x.c.x[3 * (base + at) + k];
           V[3 * at + k] = x.c.v[3 * (base + at) + k];
-          R[3 * at + k] = x.c.xold[3 * (base + at) + k];
+          R[3 * at + k] = xold[3 * (base + at) + k];
           Xd[3 * at + k] = X[3 * at + k];
         }
       }
@@ -827,6 +843,7 @@ __device__ void gas_integrate(Ctx& x, bool fused, bool eflag) {
       if (vcorr)
         for (int q = 0; q < 3 * ag; q++) V[q] += (X[q] - Xd[q]) / dt;
     }
+    if (!isfinite(X[0] + X[1] + X[2] + V[0] + V[1] + V[2])) set_status(x, MDN_ST_NONFINITE);
     bool near = fused ? (a->near_gi[gmol(P, par, s)] >= 0) : true;
     if (!near) {
       if (intra) {
@@ -987,7 +1004,10 @@ __device__ void gas_near_pass(Ctx& x, bool eflag, bool kick) {
     if (lane == 0) {
       double Fd[3 * MDN_MAX_GAS_ATOMS];
       for (int at = 0; at < ag; at++)
-        for (int k = 0; k < 3; k++) Fd[3 * at + k] = (double)F[at][k] * MDN_FIX_INV;
+        for (int k = 0; k < 3; k++) {
+          Fd[3 * at + k] = (double)F[at][k] * MDN_FIX_INV;
+          if (!(fabs(Fd[3 * at + k]) < MDN_FIX_LIMIT)) set_status(x, MDN_ST_FIXED_OVERFLOW);
+        }
       if (intra) {
         double ei = gas_intra(x, X, Fd);
         if (eflag) eintra += efixd(ei);
@@ -1030,11 +1050,11 @@ __device__ void core_reduce(Ctx& x, cg::cluster_group& cl) {
     for (int q = threadIdx.x; q < n3; q += blockDim.x) x.c.f[q] = (double)mine[q] * MDN_FIX_INV;
   }
   __syncthreads();
-  /* flag forces outside the fixed-point range or non-finite */
+  /* flag saturated forces, and positions that are no longer finite */
   if (x.rank == 0)
     for (int q = threadIdx.x; q < n3; q += blockDim.x) {
-      double f = x.c.f[q];
-      if (!(fabs(f) < MDN_FIX_LIMIT)) set_status(x, MDN_ST_FIXED_OVERFLOW);
+      if (!(fabs(x.c.f[q]) < MDN_FIX_LIMIT)) set_status(x, MDN_ST_FIXED_OVERFLOW);
+      if (!isfinite(x.c.x[q]) || !isfinite(x.c.v[q])) set_status(x, MDN_ST_NONFINITE);
     }
   x.buf ^= 1;  /* the next evaluation accumulates into the other buffer */
 }
@@ -1048,21 +1068,64 @@ __device__ void zero_acc(Ctx& x) {
 /* all forces of the step (after positions and lists are final) and the second kick */
 __device__ void forces_and_kick(Ctx& x, cg::cluster_group& cl, bool eflag, bool kick) {
   zero_acc(x);
+  prof_start(x);
   gas_near_pass(x, eflag, kick);
+  __syncthreads();
+  prof_end(x, MDN_PROF_NEAR);
+  prof_start(x);
   core_bonded(x, eflag);
+  __syncthreads();
+  prof_end(x, MDN_PROF_BONDED);
+  prof_start(x);
   core_pairs(x, eflag);
   __syncthreads();
+  prof_end(x, MDN_PROF_PAIRS);
+  prof_start(x);
   core_reduce(x, cl);
   if (kick) {
     core_kick(x);
     __syncthreads();
   }
+  prof_end(x, MDN_PROF_REDUCE);
 }
 
 /* ------------------------------------------------------------------------- */
 /* the effective-domain rebuild (MD::make_pair)                               */
 /* ------------------------------------------------------------------------- */
-__device__ void insert_gas(const Ctx& x, int q, int n_rebuild, double* X, double* V) {
+/* Philox word of insertion draw `t` (word 1 is the N2 spin) */
+__device__ __forceinline__ int insert_word(int t) { return t == 0 ? 0 : 1 + t; }
+
+__device__ void insert_vapor(const Ctx& x, int q, int n_rebuild, int t, double* X, double* V);
+
+/* true when no atom of X[0..n) lies within MDN_INSERT_MIN_DIST of a core atom
+ * (ion, vapor in the domain before this rebuild) or of a vapor molecule whose
+ * entry this rebuild already accepted */
+__device__ bool insert_clear(const Ctx& x, const double* X, int n, int n_rebuild) {
+  const double d2min = MDN_INSERT_MIN_DIST * MDN_INSERT_MIN_DIST;
+  for (int i = 0; i < x.n_core; i++) {
+    const double* c = x.c.x + 3 * i;
+    for (int a = 0; a < n; a++) {
+      double dx = X[3 * a] - c[0], dy = X[3 * a + 1] - c[1], dz = X[3 * a + 2] - c[2];
+      if (dx * dx + dy * dy + dz * dz < d2min) return false;
+    }
+  }
+  const int nc = min(x.cand[64], 64);
+  for (int k = 0; k < nc; k++) {
+    const int mi = x.cand[k];
+    const int f = x.a->region[(size_t)x.P->mol_off + mi];
+    if (!(f & 1)) continue;
+    double Xv[3 * MDN_MAX_VAP_ATOMS], Vv[3 * MDN_MAX_VAP_ATOMS];
+    insert_vapor(x, mi - 1 - x.P->n_gas, n_rebuild, f >> 2, Xv, Vv);
+    for (int b = 0; b < x.P->a_v; b++)
+      for (int a = 0; a < n; a++) {
+        double dx = X[3 * a] - Xv[3 * b], dy = X[3 * a + 1] - Xv[3 * b + 1], dz = X[3 * a + 2] - Xv[3 * b + 2];
+        if (dx * dx + dy * dy + dz * dz < d2min) return false;
+      }
+  }
+  return true;
+}
+
+__device__ void insert_gas(const Ctx& x, int q, int n_rebuild, int t, double* X, double* V) {
   const RepParams* P = x.P;
   const int ag = P->a_g, mi = 1 + q;
   const double* cx = x.a->mol_x + 3 * ((size_t)P->mol_off + mi);
@@ -1082,7 +1145,7 @@ __device__ void insert_gas(const Ctx& x, int q, int n_rebuild, double* X, double
     V[0] = 0; V[1] = vy; V[2] = vzu;
     V[3] = 0; V[4] = -vy; V[5] = -vzu;
   }
-  U4 s = draw(*P, mi, n_rebuild, 1, 0);
+  U4 s = draw(*P, mi, n_rebuild, 1, insert_word(t));
   double A = u01(s.v[0]) * 2 * 3.141592653589793;
   double B = u01(s.v[1]) * 2 * 3.141592653589793;
   double Cc = u01(s.v[2]) * 2 * 3.141592653589793;
@@ -1099,12 +1162,12 @@ __device__ void insert_gas(const Ctx& x, int q, int n_rebuild, double* X, double
   }
 }
 
-__device__ void insert_vapor(const Ctx& x, int q, int n_rebuild, double* X, double* V) {
+__device__ void insert_vapor(const Ctx& x, int q, int n_rebuild, int t, double* X, double* V) {
   const RepParams* P = x.P;
   const int av = P->a_v, mi = 1 + P->n_gas + q;
   const double* cx = x.a->mol_x + 3 * ((size_t)P->mol_off + mi);
   const double* cv = x.a->mol_v + 3 * ((size_t)P->mol_off + mi);
-  U4 s = draw(*P, mi, n_rebuild, 1, 0);
+  U4 s = draw(*P, mi, n_rebuild, 1, insert_word(t));
   double A = u01(s.v[0]) * 2 * 3.141592653589793;
   double B = u01(s.v[1]) * 2 * 3.141592653589793;
   double Cc = u01(s.v[2]) * 2 * 3.141592653589793;
@@ -1121,9 +1184,13 @@ __device__ void insert_vapor(const Ctx& x, int q, int n_rebuild, double* X, doub
 }
 
 /* free flight, in/out test, wrap and resampling of one molecule; returns
- * (was_in << 1) | now_in */
+ * (draw << 2) | (was_in << 1) | now_in, draw = the insertion draw that passed
+ * the overlap test (0 under MDN_Q_BLIND_INSERT).  A molecule inside the sphere
+ * whose draws all overlap stays outside, unwrapped and not resampled, until
+ * the next rebuild.  Entering vapor molecules become candidates that
+ * vapor_entries() decides. */
 __device__ __forceinline__ int classify_one(const Ctx& x, int mi, double sigma, int n_rebuild, int loop_pair,
-                                            const double* com) {
+                                            const double* com, int kind /* 0 gas, 1 vapor */) {
   const RepParams* P = x.P;
   const size_t g = (size_t)P->mol_off + mi;
   double* X = x.a->mol_x + 3 * g;
@@ -1136,6 +1203,32 @@ __device__ __forceinline__ int classify_one(const Ctx& x, int mi, double sigma, 
   double dz = X[2] - com[2];
   double r2 = (dx * dx + dy * dy + dz * dz);
   int in = r2 < P->RI2 ? 1 : 0;
+  int draw_ok = 0;
+  if (in && !was && !(P->quirks & MDN_Q_BLIND_INSERT) && kind == 1) {
+    /* decided by vapor_entries(): recorded as a candidate, provisionally in;
+     * beyond 64 candidates in one rebuild the entry waits for the next */
+    int c = atomicAdd(&x.cand[64], 1);
+    if (c >= 64) {
+      x.a->region[g] = 0;
+      return 0;
+    }
+    x.cand[c] = mi;
+    x.a->region[g] = (unsigned char)1;
+    return 1;
+  }
+  if (in && !was && !(P->quirks & MDN_Q_BLIND_INSERT)) {
+    double Xt[3 * MDN_MAX_VAP_ATOMS], Vt[3 * MDN_MAX_VAP_ATOMS];
+    int t = 0;
+    for (; t < MDN_INSERT_TRIES; t++) {
+      insert_gas(x, mi - 1, n_rebuild, t, Xt, Vt);
+      if (insert_clear(x, Xt, P->a_g, n_rebuild)) break;
+    }
+    if (t == MDN_INSERT_TRIES) {
+      x.a->region[g] = 0; /* the entry waits for the next rebuild */
+      return 0;
+    }
+    draw_ok = t;
+  }
   if (!in) {
     double HL = P->box * 0.5;
     if (dx < -HL) X[0] += P->box;
@@ -1152,8 +1245,8 @@ __device__ __forceinline__ int classify_one(const Ctx& x, int mi, double sigma, 
     V[1] = z1 * sigma;
     V[2] = z2 * sigma;
   }
-  x.a->region[g] = (unsigned char)((was << 1) | in);
-  return (was << 1) | in;
+  x.a->region[g] = (unsigned char)((draw_ok << 2) | (was << 1) | in);
+  return (draw_ok << 2) | (was << 1) | in;
 }
 
 /* exchange one int per CTA across the cluster: returns the prefix before this
@@ -1289,6 +1382,66 @@ __device__ void relist(Ctx& x, cg::cluster_group& cl) {
   cl.sync();
 }
 
+/* The overlap test of entering vapor molecules: against the ion, the vapor
+ * already in the domain and every in-domain gas atom (up to ~20,000), so the
+ * whole block tests each candidate's draws.  Rank 0 only; returns the number
+ * of entries that must wait. */
+__device__ int vapor_entries(Ctx& x, int nreb) {
+  const RepParams* P = x.P;
+  const KArgs* a = x.a;
+  const int av = P->a_v, ag = P->a_g, par = x.D->parity, G = x.D->n_gas_in;
+  const double d2min = MDN_INSERT_MIN_DIST * MDN_INSERT_MIN_DIST;
+  const int nc = min(x.cand[64], 64);
+  int deferred = 0;
+  for (int c = 0; c < nc; c++) {
+    const int mi = x.cand[c];
+    const int q = mi - 1 - P->n_gas;
+    int t = 0;
+    for (; t < MDN_INSERT_TRIES; t++) {
+      if (threadIdx.x == 0) {
+        double V[3 * MDN_MAX_VAP_ATOMS];
+        insert_vapor(x, q, nreb, t, x.trial, V);
+        x.iscr[51] = 1;
+      }
+      __syncthreads();
+      bool clash = false;
+      for (int i = threadIdx.x; i < x.n_core && !clash; i += blockDim.x) {
+        const double* cpos = x.c.x + 3 * i;
+        for (int k = 0; k < av; k++) {
+          double dx = x.trial[3 * k] - cpos[0], dy = x.trial[3 * k + 1] - cpos[1], dz = x.trial[3 * k + 2] - cpos[2];
+          if (dx * dx + dy * dy + dz * dz < d2min) clash = true;
+        }
+      }
+      for (int u = threadIdx.x; u < G * ag && !clash; u += blockDim.x) {
+        const double* gp = a->slab_x + 3 * ((size_t)P->slab_off + (size_t)par * P->slab_cap * ag + u);
+        for (int k = 0; k < av; k++) {
+          double dx = x.trial[3 * k] - gp[0], dy = x.trial[3 * k + 1] - gp[1], dz = x.trial[3 * k + 2] - gp[2];
+          if (dx * dx + dy * dy + dz * dz < d2min) clash = true;
+        }
+      }
+      if (clash) x.iscr[51] = 0;
+      __syncthreads();
+      int ok = x.iscr[51];
+      __syncthreads();
+      if (ok) break;
+    }
+    if (threadIdx.x == 0) {
+      size_t g = (size_t)P->mol_off + mi;
+      if (t == MDN_INSERT_TRIES) {
+        a->region[g] = 0; /* the entry waits for the next rebuild */
+        deferred++;
+      } else {
+        a->region[g] = (unsigned char)((t << 2) | 1);
+      }
+    }
+  }
+  if (threadIdx.x == 0) x.iscr[52] = deferred;
+  __syncthreads();
+  int d = x.iscr[52];
+  __syncthreads();
+  return d;
+}
+
 __device__ void make_pair(Ctx& x, cg::cluster_group& cl) {
   const RepParams* P = x.P;
   const KArgs* a = x.a;
@@ -1350,21 +1503,15 @@ __device__ void make_pair(Ctx& x, cg::cluster_group& cl) {
   }
   __threadfence();
   cl.sync();
-  /* free flight + classification of the gas molecules of this CTA's range */
   double com[3] = {x.D->ion_com[0], x.D->ion_com[1], x.D->ion_com[2]};
   int mlo, mhi;
   partition(x, P->n_gas, &mlo, &mhi);
   int my_in = 0;
   double vmax2 = 0;
-  for (int q = mlo + threadIdx.x; q < mhi; q += blockDim.x) {
-    int f = classify_one(x, 1 + q, P->gas_sigma, nreb, loop_pair, com);
-    my_in += f & 1;
-    const double* V = a->mol_v + 3 * ((size_t)P->mol_off + 1 + q);
-    double v2 = V[0] * V[0] + V[1] * V[1] + V[2] * V[2];
-    vmax2 = fmax(vmax2, v2);
-  }
   /* vapor molecules (rank 0; events) */
   int my_vin = 0;
+  if (threadIdx.x == 0) x.cand[64] = 0;
+  __syncthreads();
   if (x.rank == 0)
     for (int q = threadIdx.x; q < P->n_vap; q += blockDim.x) {
       int mi = 1 + P->n_gas + q;
@@ -1390,18 +1537,35 @@ __device__ void make_pair(Ctx& x, cg::cluster_group& cl) {
           set_status(x, MDN_ST_EVENT_OVERFLOW);
         }
       }
-      int f = classify_one(x, mi, P->vap_sigma, nreb, loop_pair, com);
+      int f = classify_one(x, mi, P->vap_sigma, nreb, loop_pair, com, 1);
       my_vin += f & 1;
       const double* V = a->mol_v + 3 * g;
       double v2 = V[0] * V[0] + V[1] * V[1] + V[2] * V[2];
       vmax2 = fmax(vmax2, v2);
     }
+  /* the vapor decisions (and their accepted draws) before any gas entry is
+   * tested against them: every CTA takes rank 0's candidate list */
+  my_vin = block_sum_i(my_vin, sc);
+  if (x.rank == 0 && !(P->quirks & MDN_Q_BLIND_INSERT)) my_vin -= vapor_entries(x, nreb);
+  __threadfence();
+  cl.sync();
+  if (x.rank != 0) {
+    for (int k = threadIdx.x; k <= 64; k += blockDim.x) x.cand[k] = *cl.map_shared_rank(&x.cand[k], 0);
+  }
+  __syncthreads();
+  /* free flight + classification of the gas molecules of this CTA's range */
+  for (int q = mlo + threadIdx.x; q < mhi; q += blockDim.x) {
+    int f = classify_one(x, 1 + q, P->gas_sigma, nreb, loop_pair, com, 0);
+    my_in += f & 1;
+    const double* V = a->mol_v + 3 * ((size_t)P->mol_off + 1 + q);
+    double v2 = V[0] * V[0] + V[1] * V[1] + V[2] * V[2];
+    vmax2 = fmax(vmax2, v2);
+  }
   {
     const double* V = x.D->ion_com + 3;
     vmax2 = fmax(vmax2, V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
   }
   my_in = block_sum_i(my_in, sc);
-  my_vin = block_sum_i(my_vin, sc);
   vmax2 = block_max_d(vmax2, x.dscr);
   __threadfence();
   int gin_base, gin_tot, vin_base, vin_tot;
@@ -1438,7 +1602,7 @@ __device__ void make_pair(Ctx& x, cg::cluster_group& cl) {
             }
           }
         } else {
-          insert_gas(x, q, nreb, X, V);
+          insert_gas(x, q, nreb, f >> 2, X, V);
         }
         for (int at = 0; at < ag; at++) {
           size_t gn = gatom(P, npar, ns, at);
@@ -1482,7 +1646,7 @@ __device__ void make_pair(Ctx& x, cg::cluster_group& cl) {
               }
             }
           } else {
-            insert_vapor(x, q, nreb, X, V);
+            insert_vapor(x, q, nreb, f >> 2, X, V);
           }
           for (int at = 0; at < av; at++) {
             size_t gn = vatom(P, npar, ns, at);
@@ -1529,6 +1693,7 @@ __device__ void make_pair(Ctx& x, cg::cluster_group& cl) {
 /* ------------------------------------------------------------------------- */
 __device__ void one_step(Ctx& x, cg::cluster_group& cl, bool eflag) {
   const RepParams* P = x.P;
+  prof_start(x);
   core_kick(x);
   __syncthreads();
   if (x.D->nvt_mode == MDN_NVT_SCALE) {
@@ -1549,16 +1714,21 @@ __device__ void one_step(Ctx& x, cg::cluster_group& cl, bool eflag) {
     __syncthreads();
   }
   core_weights_pos(x, true);
+  prof_end(x, MDN_PROF_CORE_INT);
+  prof_start(x);
   const bool rebuild = x.D->loop_pair + 1 > x.D->loop_update;
   gas_integrate(x, !rebuild, eflag);
   __threadfence_block();
   __syncthreads();
   if (threadIdx.x == 0) x.D->loop_pair += 1;
   __syncthreads();
+  prof_end(x, MDN_PROF_GAS_INT);
   if (rebuild) {
+    prof_start(x);
     make_pair(x, cl);
     gas_far_pass(x, eflag, true);
     __syncthreads();
+    prof_end(x, MDN_PROF_REBUILD);
   }
   forces_and_kick(x, cl, eflag, true);
   if (x.D->nvt_mode == MDN_NVT_NH) {
@@ -1581,6 +1751,8 @@ extern "C" __global__ void __launch_bounds__(512, 1) mdn_advance(KArgs a) {
   __shared__ int s_job;
   __shared__ int iscr[64];
   __shared__ double dscr[64];
+  __shared__ int cand[65];
+  __shared__ double trial[3 * MDN_MAX_VAP_ATOMS];
 
   Ctx x;
   x.a = &a;
@@ -1590,6 +1762,8 @@ extern "C" __global__ void __launch_bounds__(512, 1) mdn_advance(KArgs a) {
   x.C = (int)cl.num_blocks();
   x.iscr = iscr;
   x.dscr = dscr;
+  x.cand = cand;
+  x.trial = trial;
   /* carve the dynamic shared memory */
   {
     unsigned char* p = dsm;
@@ -1599,7 +1773,6 @@ extern "C" __global__ void __launch_bounds__(512, 1) mdn_advance(KArgs a) {
     x.c.x = (double*)take(sizeof(double) * 3 * nc);
     x.c.v = (double*)take(sizeof(double) * 3 * nc);
     x.c.f = (double*)take(sizeof(double) * 3 * nc);
-    x.c.xold = (double*)take(sizeof(double) * 3 * nc);
     x.c.pos = (float4*)take(sizeof(float4) * nc);
     x.c.w = (float*)take(sizeof(float) * nc);
     x.c.type = (int*)take(sizeof(int) * nc);
@@ -1621,12 +1794,13 @@ extern "C" __global__ void __launch_bounds__(512, 1) mdn_advance(KArgs a) {
     if (threadIdx.x == 0) {
       sP = a.P[r];
       sD = a.D[r];
+      sD.nvt_mode = a.ctl_mode[r];
+      sD.nvt_T = a.ctl_T[r];
     }
     __syncthreads();
     x.ib = a.iblob + sP.iblob_off;
     x.db = a.dblob + sP.dblob_off;
-    const bool fatal =
-        (a.status[r] & (MDN_ST_SLAB_OVERFLOW | MDN_ST_CORE_OVERFLOW | MDN_ST_LIST_OVERFLOW)) != 0;
+    const bool fatal = (a.status[r] & MDN_ST_FATAL) != 0;
     const bool fits = sP.n_types <= a.nt_cap && sP.n_ion * sP.excl_words <= a.excl_cap &&
                       sP.n_ion + sD.n_vap_in * sP.a_v <= a.nc_cap;
     if (fatal || !fits) {
@@ -1644,7 +1818,9 @@ extern "C" __global__ void __launch_bounds__(512, 1) mdn_advance(KArgs a) {
     for (int q = threadIdx.x; q < sP.n_ion * sP.excl_words; q += blockDim.x) x.c.excl[q] = (unsigned)x.ib[sP.o_excl + q];
     load_ion(x);
     load_vapor(x);
+    if (threadIdx.x < MDN_PROF_N) s_prof[threadIdx.x] = 0;
     __syncthreads();
+    const long long job_t0 = clock64();
     if (a.mode == MDN_MODE_STEP) {
       for (long long s = 0; s < a.n_steps; s++) {
         bool eflag = a.energy_mode == 2 || (a.energy_mode == 1 && s == a.n_steps - 1);
@@ -1670,6 +1846,11 @@ extern "C" __global__ void __launch_bounds__(512, 1) mdn_advance(KArgs a) {
       relist(x, cl);
     }
     __syncthreads();
+    if (a.prof && threadIdx.x == 0) {
+      s_prof[MDN_PROF_TOTAL] = clock64() - job_t0;
+      for (int k = 0; k < MDN_PROF_N; k++)
+        atomicAdd((unsigned long long*)&a.prof[(size_t)r * MDN_PROF_N + k], (unsigned long long)s_prof[k]);
+    }
     store_core(x);
     __syncthreads();
     if (x.rank == 0 && threadIdx.x == 0) {

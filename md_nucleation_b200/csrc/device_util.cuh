@@ -69,8 +69,14 @@ __device__ __forceinline__ void rotation(double& X, double& Y, double& Z, double
   Z = x * sB - y * sA * cB + z * cA * cB;
 }
 
-__device__ __forceinline__ long long fixd(double f) { return __double2ll_rn(f * MDN_FIX_SCALE); }
-__device__ __forceinline__ long long fixf(float f) { return __float2ll_rn(f * 1099511627776.0f); }
+/* fixed-point conversion of one term, saturated at +-2^21 kcal/mol/A so that a
+ * few saturated terms still sum inside int64 (NaN converts to 0) */
+__device__ __forceinline__ long long fixd(double f) {
+  return __double2ll_rn(fmin(fmax(f, -2097152.0), 2097152.0) * MDN_FIX_SCALE);
+}
+__device__ __forceinline__ long long fixf(float f) {
+  return __float2ll_rn(fminf(fmaxf(f, -2097152.0f), 2097152.0f) * 1099511627776.0f);
+}
 __device__ __forceinline__ long long efixd(double e) { return __double2ll_rn(e * MDN_EFIX_SCALE); }
 __device__ __forceinline__ long long efixf(float e) { return __float2ll_rn(e * 68719476736.0f); }
 

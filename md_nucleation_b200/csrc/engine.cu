@@ -25,6 +25,10 @@
 #include "mdn_types.h"
 
 extern "C" __global__ void mdn_advance(KArgs a);
+int mdn_snapshot_device(const RepParams* dP, const RepDyn* dD, const int* d_iblob, int R, const double* ion_x,
+                        const double* ion_v, const double* slab_x, const double* slab_v, const double* vslab_x,
+                        const double* vslab_v, long long* d_offset, int* d_type, double* d_x, double* d_v,
+                        long long d_capacity, cudaStream_t stream);
 
 namespace {
 
@@ -126,11 +130,22 @@ struct mdn_handle {
   int* job_counter = nullptr;
   std::vector<int> order;
   std::vector<int> h_iblob;
+  std::vector<int> ctl_mode;
+  std::vector<double> ctl_T;
+  int* d_ctl_mode = nullptr;
+  double* d_ctl_T = nullptr;
+  long long* d_prof = nullptr;
+  bool prof_on = false;
   /* sizes */
   size_t n_ion_tot = 0, n_mol_tot = 0, n_slab_atoms = 0, n_slab_mols = 0, n_vslab_atoms = 0,
          n_vslab_mols = 0, n_near = 0, n_gil = 0, n_gvl = 0;
   double last_ms = 0;
   long long last_launches = 0;
+  /* snapshot staging */
+  long long snap_cap = 0;
+  long long* snap_off = nullptr;
+  int* snap_type = nullptr;
+  double *snap_x = nullptr, *snap_v = nullptr;
   std::vector<std::vector<std::string>> names;
 };
 
@@ -141,7 +156,8 @@ void free_all(mdn_handle* h) {
                   h->region, h->slot, h->slab_x, h->slab_v, h->slab_f, h->slab_mol, h->vslab_x, h->vslab_v,
                   h->vslab_f, h->vslab_w, h->vslab_mol, h->near_list, h->near_gi, h->near_gv, h->gil_n,
                   h->gvl_n, h->gil, h->gvl, h->energy, h->events, h->n_events, h->status, h->job_order,
-                  h->job_counter};
+                  h->job_counter, h->snap_off, h->snap_type, h->snap_x, h->snap_v, h->d_ctl_mode,
+                  h->d_ctl_T, h->d_prof};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -155,7 +171,7 @@ size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
 size_t smem_bytes(int nc, int nt, int excl) {
   size_t s = 0;
   s += align16(sizeof(long long) * 6 * nc);
-  s += 4 * align16(sizeof(double) * 3 * nc);
+  s += 3 * align16(sizeof(double) * 3 * nc);
   s += align16(sizeof(float4) * nc);
   s += 3 * align16(sizeof(int) * nc);
   s += align16(sizeof(unsigned) * excl);
@@ -214,6 +230,8 @@ long long launch(mdn_handle* h, int mode, long long n_steps, int energy_mode, un
   a.energy = h->energy;
   a.events = h->events; a.n_events = h->n_events; a.ev_cap = h->ev_cap;
   a.status = h->status;
+  a.ctl_mode = h->d_ctl_mode;
+  a.ctl_T = h->d_ctl_T;
   a.job_order = h->job_order;
   a.n_jobs = (int)J.size();
   a.job_counter = h->job_counter;
@@ -222,6 +240,7 @@ long long launch(mdn_handle* h, int mode, long long n_steps, int energy_mode, un
   a.mode = mode;
   a.term_mask = term_mask;
   a.keep_com = keep_com;
+  a.prof = h->prof_on ? h->d_prof : nullptr;
   a.nc_cap = h->nc_cap;
   a.nt_cap = h->nt_cap;
   a.excl_cap = h->excl_cap;
@@ -476,8 +495,12 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
     double eg = d.n_gas * frac;
     P.slab_cap = (int)std::min<double>(d.n_gas, ceil(eg * f + 6 * sqrt(eg) + 64));
     P.slab_cap = std::max(P.slab_cap, 1);
+    /* in-domain vapor: binomial mean + 4 sigma (the core lives in shared memory,
+     * 148 B per atom, so this capacity is kept tight; exceeding it raises
+     * MDN_ST_CORE_OVERFLOW) */
     double ev = d.n_vapor * frac;
-    P.vcap = (int)std::min<double>(d.n_vapor, ceil(ev * 2 * f + 6 * sqrt(ev) + 16));
+    P.vcap = (int)std::min<double>(d.n_vapor, ceil(ev * (f > 1.0 ? 1.0 + 0.2 * (f - 1.0) : 1.0) +
+                                                   4 * sqrt(ev * (1 - frac)) + 8));
     P.vcap = std::max(P.vcap, 1);
     P.near_cap = P.slab_cap;
     double rion = 0;
@@ -540,9 +563,10 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
   cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->dev);
   if (h->smem + 4096 > (size_t)max_optin) {
     size_t need = h->smem;
+    int nc = h->nc_cap;
     delete h;
-    return fail(MDN_ERR_CAPACITY, "core of %d atoms needs %zu B of shared memory (device limit %d)",
-                0, need, max_optin);
+    return fail(MDN_ERR_CAPACITY, "a core of %d atoms needs %zu B of shared memory (device limit %d)",
+                nc, need, max_optin);
   }
   h->n_ion_tot = ion_tot;
   h->n_mol_tot = mol_tot;
@@ -601,6 +625,8 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
   ALLOC(h->status, R);
   ALLOC(h->job_order, R);
   ALLOC(h->job_counter, 1);
+  ALLOC(h->d_ctl_mode, R);
+  ALLOC(h->d_ctl_T, R);
 #undef ALLOC
   int rc = MDN_OK;
   auto ck = [&](cudaError_t e, const char* what) {
@@ -626,6 +652,14 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
   ck(cudaMemset(h->n_events, 0, sizeof(int)), "events");
   ck(cudaMemset(h->status, 0, sizeof(int) * R), "status");
   ck(cudaMemset(h->near_gi, 0xff, sizeof(int) * slab_mols), "near_gi");
+  h->ctl_mode.resize(R);
+  h->ctl_T.resize(R);
+  for (int r = 0; r < R; r++) {
+    h->ctl_mode[r] = descs[r].nvt_mode;
+    h->ctl_T[r] = descs[r].nvt_temperature;
+  }
+  ck(cudaMemcpy(h->d_ctl_mode, h->ctl_mode.data(), sizeof(int) * R, cudaMemcpyHostToDevice), "ctl");
+  ck(cudaMemcpy(h->d_ctl_T, h->ctl_T.data(), sizeof(double) * R, cudaMemcpyHostToDevice), "ctl");
   /* ion atoms and molecule centres */
   {
     std::vector<double> ix(3 * ion_tot), iv(3 * ion_tot), mx(3 * mol_tot, 0.0), mv(3 * mol_tot, 0.0);
@@ -682,7 +716,7 @@ static int check_status(mdn_handle* h) {
   cudaError_t e = cudaMemcpy(st.data(), h->status, sizeof(int) * h->R, cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return fail(MDN_ERR_CUDA, "status read: %s", cudaGetErrorString(e));
   for (int r = 0; r < h->R; r++)
-    if (st[r]) return fail(MDN_ERR_REPLICA, "replica %d raised status 0x%x", r, st[r]);
+    if (st[r] & MDN_ST_FATAL) return fail(MDN_ERR_REPLICA, "replica %d raised status 0x%x", r, st[r]);
   return MDN_OK;
 }
 
@@ -778,14 +812,27 @@ int mdn_recenter(mdn_handle* h, int compat) {
 
 int mdn_set_nvt(mdn_handle* h, int replica, int mode, double T) {
   if (!h || replica >= h->R) return fail(MDN_ERR_ARG, "bad replica");
+  if (mode < MDN_NVT_OFF || mode > MDN_NVT_NH) return fail(MDN_ERR_ARG, "bad thermostat mode");
   for (int r = 0; r < h->R; r++) {
     if (replica >= 0 && r != replica) continue;
-    RepDyn D;
-    CK(cudaMemcpy(&D, h->dD + r, sizeof D, cudaMemcpyDeviceToHost));
-    D.nvt_mode = mode;
-    D.nvt_T = T;
-    CK(cudaMemcpy(h->dD + r, &D, sizeof D, cudaMemcpyHostToDevice));
+    h->ctl_mode[r] = mode;
+    h->ctl_T[r] = T;
   }
+  CK(cudaMemcpy(h->d_ctl_mode, h->ctl_mode.data(), sizeof(int) * h->R, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_ctl_T, h->ctl_T.data(), sizeof(double) * h->R, cudaMemcpyHostToDevice));
+  return MDN_OK;
+}
+
+int mdn_set_nvt_batch(mdn_handle* h, const int* mode, const double* T) {
+  if (!h || !mode || !T) return fail(MDN_ERR_ARG, "bad arguments");
+  for (int r = 0; r < h->R; r++) {
+    if (mode[r] < MDN_NVT_OFF || mode[r] > MDN_NVT_NH) return fail(MDN_ERR_ARG, "bad thermostat mode");
+    h->ctl_mode[r] = mode[r];
+    h->ctl_T[r] = T[r];
+  }
+  cudaSetDevice(h->dev);
+  CK(cudaMemcpyAsync(h->d_ctl_mode, mode, sizeof(int) * h->R, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_ctl_T, T, sizeof(double) * h->R, cudaMemcpyHostToDevice, h->stream));
   return MDN_OK;
 }
 
@@ -1076,6 +1123,54 @@ int mdn_in_domain(mdn_handle* h, int r, int capacity, int* count, int* type, dou
   return MDN_OK;
 }
 
+int mdn_snapshot(mdn_handle* h, long long* offset, long long capacity, int* type, double* x, double* v,
+                 double* U) {
+  if (!h || !offset) return fail(MDN_ERR_ARG, "bad arguments");
+  cudaSetDevice(h->dev);
+  if (!h->snap_off) {
+    long long cap = 0;
+    for (int r = 0; r < h->R; r++) {
+      const RepParams& P = h->P[r];
+      cap += P.n_ion + (long long)P.slab_cap * P.a_g + (P.n_vap > 0 ? (long long)P.vcap * P.a_v : 0);
+    }
+    h->snap_cap = cap;
+    CK(cudaMalloc((void**)&h->snap_off, sizeof(long long) * (h->R + 1)));
+    CK(cudaMalloc((void**)&h->snap_type, sizeof(int) * std::max<long long>(cap, 1)));
+    CK(cudaMalloc((void**)&h->snap_x, 3 * sizeof(double) * std::max<long long>(cap, 1)));
+    CK(cudaMalloc((void**)&h->snap_v, 3 * sizeof(double) * std::max<long long>(cap, 1)));
+  }
+  if (mdn_snapshot_device(h->dP, h->dD, h->d_iblob, h->R, h->ion_x, h->ion_v, h->slab_x, h->slab_v, h->vslab_x,
+                          h->vslab_v, h->snap_off, h->snap_type, h->snap_x, h->snap_v, h->snap_cap, h->stream))
+    return fail(MDN_ERR_CUDA, "snapshot kernels: %s", cudaGetErrorString(cudaGetLastError()));
+  CK(cudaMemcpyAsync(offset, h->snap_off, sizeof(long long) * (h->R + 1), cudaMemcpyDeviceToHost, h->stream));
+  std::vector<long long> e(U ? 8 * h->R : 0);
+  if (U) CK(cudaMemcpyAsync(e.data(), h->energy, sizeof(long long) * e.size(), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (U)
+    for (size_t i = 0; i < e.size(); i++) U[i] = (double)e[i] * MDN_EFIX_INV;
+  const long long total = offset[h->R];
+  if (total > capacity) return fail(MDN_ERR_CAPACITY, "snapshot needs %lld rows, buffer holds %lld", total, capacity);
+  if (total > 0) {
+    if (type) CK(cudaMemcpyAsync(type, h->snap_type, sizeof(int) * total, cudaMemcpyDeviceToHost, h->stream));
+    if (x) CK(cudaMemcpyAsync(x, h->snap_x, 3 * sizeof(double) * total, cudaMemcpyDeviceToHost, h->stream));
+    if (v) CK(cudaMemcpyAsync(v, h->snap_v, 3 * sizeof(double) * total, cudaMemcpyDeviceToHost, h->stream));
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  return MDN_OK;
+}
+
+int mdn_host_alloc(size_t bytes, void** ptr) {
+  if (!ptr) return fail(MDN_ERR_ARG, "null pointer");
+  *ptr = nullptr;
+  CK(cudaHostAlloc(ptr, std::max<size_t>(bytes, 1), cudaHostAllocDefault));
+  return MDN_OK;
+}
+
+int mdn_host_free(void* ptr) {
+  if (ptr) CK(cudaFreeHost(ptr));
+  return MDN_OK;
+}
+
 int mdn_events(mdn_handle* h, mdn_event* ev, int capacity, int* count) {
   if (!h || !count) return fail(MDN_ERR_ARG, "bad arguments");
   int n = 0;
@@ -1146,6 +1241,22 @@ int mdn_last_timing(mdn_handle* h, double* ms, long long* launches) {
   if (!h) return fail(MDN_ERR_ARG, "null handle");
   if (ms) *ms = h->last_ms;
   if (launches) *launches = h->last_launches;
+  return MDN_OK;
+}
+
+int mdn_profile(mdn_handle* h, int enable, long long* out) {
+  if (!h) return fail(MDN_ERR_ARG, "null handle");
+  cudaSetDevice(h->dev);
+  if (!h->d_prof) {
+    CK(cudaMalloc((void**)&h->d_prof, sizeof(long long) * MDN_PROF_N * h->R));
+    CK(cudaMemset(h->d_prof, 0, sizeof(long long) * MDN_PROF_N * h->R));
+  }
+  if (out) {
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpy(out, h->d_prof, sizeof(long long) * MDN_PROF_N * h->R, cudaMemcpyDeviceToHost));
+  }
+  if (enable && !h->prof_on) CK(cudaMemset(h->d_prof, 0, sizeof(long long) * MDN_PROF_N * h->R));
+  h->prof_on = enable != 0;
   return MDN_OK;
 }
 

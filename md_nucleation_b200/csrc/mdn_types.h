@@ -36,7 +36,18 @@
 #define MDN_FIX_INV (1.0 / 1099511627776.0)
 #define MDN_EFIX_SCALE 68719476736.0
 #define MDN_EFIX_INV (1.0 / 68719476736.0)
-#define MDN_FIX_LIMIT 8.0e6 /* |force component| above this flags a fixed-point overflow */
+#define MDN_FIX_LIMIT 2.0e6 /* |force component| above this flags saturation (a warning) */
+
+/* phases of the per-replica cycle accounting (mdn_profile) */
+#define MDN_PROF_TOTAL 0
+#define MDN_PROF_CORE_INT 1   /* kick, thermostat, drift, SHAKE, centre, weights */
+#define MDN_PROF_GAS_INT 2    /* gas kick/drift (+ far-molecule forces)          */
+#define MDN_PROF_REBUILD 3    /* make_pair                                       */
+#define MDN_PROF_NEAR 4       /* near gas molecules: gas-ion, gas-vapor          */
+#define MDN_PROF_BONDED 5     /* core bonded terms                               */
+#define MDN_PROF_PAIRS 6      /* core pair terms                                 */
+#define MDN_PROF_REDUCE 7     /* core force sums, core kick                      */
+#define MDN_PROF_N 8
 
 /* kernel modes */
 #define MDN_MODE_STEP 0       /* advance n_steps                                   */
@@ -117,6 +128,8 @@ typedef struct KArgs {
   int* n_events;
   int ev_cap;
   int* status;             /* [n_replicas] MDN_ST_* bits, only ever OR-ed      */
+  const int* ctl_mode;     /* [n_replicas] thermostat mode (MDN_NVT_*)         */
+  const double* ctl_T;     /* [n_replicas] thermostat target (K)               */
   const int* job_order;
   int n_jobs;
   int* job_counter;
@@ -124,6 +137,7 @@ typedef struct KArgs {
   int energy_mode, mode;
   int keep_com;            /* MAKE_PAIR: classify against the stored ion centre */
   unsigned term_mask;
+  long long* prof;         /* NULL, or [n_replicas][MDN_PROF_N] SM cycles per phase */
   int nc_cap;              /* core atoms the shared memory holds               */
   int nt_cap;              /* atom types the shared memory holds               */
   int excl_cap;            /* exclusion words the shared memory holds          */

@@ -61,6 +61,12 @@ def lib():
         L.mdn_kinetic.argtypes = [vp, C.POINTER(C.c_double)]
         L.mdn_last_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
         L.mdn_set_launch.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+        L.mdn_snapshot.argtypes = [vp, C.POINTER(C.c_longlong), C.c_longlong, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.POINTER(C.c_double)]
+        L.mdn_host_alloc.argtypes = [C.c_size_t, C.POINTER(C.c_void_p)]
+        L.mdn_host_free.argtypes = [C.c_void_p]
+        L.mdn_set_nvt_batch.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+        L.mdn_profile.argtypes = [vp, C.c_int, C.POINTER(C.c_longlong)]
         if L.mdn_abi_version() != abi.ABI_VERSION:
             raise RuntimeError("libmdn.so ABI version mismatch")
         _LIB = L
@@ -84,6 +90,58 @@ def default_options(**kw) -> abi.Options:
     for k, v in kw.items():
         setattr(o, k, v)
     return o
+
+
+class PinnedArray:
+    """A numpy view of page-locked host memory from mdn_host_alloc."""
+
+    def __init__(self, shape, dtype):
+        self.nbytes = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        self.ptr = C.c_void_p()
+        _ck(lib().mdn_host_alloc(self.nbytes, C.byref(self.ptr)))
+        buf = (C.c_byte * self.nbytes).from_address(self.ptr.value)
+        self.array = np.frombuffer(buf, dtype=dtype).reshape(shape)
+
+    def free(self):
+        if self.ptr:
+            lib().mdn_host_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class SnapshotBuffer:
+    """Host buffers of mdn_snapshot (page-locked when pinned=True)."""
+
+    def __init__(self, n_replicas: int, capacity: int, pinned: bool = True):
+        self.capacity = int(capacity)
+        self.offset = np.zeros(n_replicas + 1, np.int64)
+        if pinned:
+            self._t = PinnedArray((capacity,), np.int32)
+            self._x = PinnedArray((capacity, 3), np.float64)
+            self._v = PinnedArray((capacity, 3), np.float64)
+            self.type, self.x, self.v = self._t.array, self._x.array, self._v.array
+        else:
+            self.type = np.zeros(capacity, np.int32)
+            self.x = np.zeros((capacity, 3))
+            self.v = np.zeros((capacity, 3))
+        self.type_ptr = self.type.ctypes.data_as(C.c_void_p)
+        self.x_ptr = self.x.ctypes.data_as(C.c_void_p)
+        self.v_ptr = self.v.ctypes.data_as(C.c_void_p)
+        self.U = None
+
+    def rows(self, r):
+        a, b = self.offset[r], self.offset[r + 1]
+        return self.type[a:b], self.x[a:b], self.v[a:b]
+
+    @property
+    def nbytes_used(self):
+        n = int(self.offset[-1])
+        return n * (4 + 48)
 
 
 class Engine:
@@ -131,6 +189,9 @@ class Engine:
 
     def set_nvt(self, mode: int, temperature: float = 300.0, replica: int = -1):
         _ck(self.L.mdn_set_nvt(self.h, replica, mode, temperature))
+
+    def set_nvt_batch(self, modes: np.ndarray, temperatures: np.ndarray):
+        _ck(self.L.mdn_set_nvt_batch(self.h, abi.ptr(modes, C.c_int), abi.ptr(temperatures)))
 
     def compute_forces(self, term_mask: int = 0):
         _ck(self.L.mdn_compute_forces(self.h, term_mask))
@@ -195,6 +256,25 @@ class Engine:
     def kinetic(self) -> np.ndarray:
         out = np.zeros((self.n, 4))
         _ck(self.L.mdn_kinetic(self.h, abi.ptr(out)))
+        return out
+
+    def snapshot(self, buf: "SnapshotBuffer", energies: bool = True):
+        """All replicas' in-domain atoms (and energies) into `buf`; returns the
+        row offsets per replica."""
+        U = np.zeros((self.n, 8)) if energies else None
+        _ck(self.L.mdn_snapshot(self.h, abi.ptr(buf.offset, C.c_longlong), buf.capacity, buf.type_ptr,
+                                buf.x_ptr, buf.v_ptr, abi.ptr(U) if energies else None))
+        buf.U = U
+        return buf.offset
+
+    PROFILE_PHASES = ("total", "core_integration", "gas_integration", "rebuild", "near_gas",
+                      "core_bonded", "core_pairs", "core_reduce_kick")
+
+    def profile(self, enable: bool = True):
+        """Starts (enable) or stops the per-replica cycle accounting; returns the
+        [n_replicas, 8] cycles accumulated so far."""
+        out = np.zeros((self.n, 8), np.int64)
+        _ck(self.L.mdn_profile(self.h, 1 if enable else 0, abi.ptr(out, C.c_longlong)))
         return out
 
     def last_timing(self):

@@ -174,11 +174,13 @@ def nacl_cluster() -> Species:
 def chain(n_atoms: int, charge: float, rng: np.random.Generator) -> Species:
     """A +q peptide-like chain: a self-avoiding heavy-atom backbone (bonds
     1.33-1.53 A, angles 110-120 deg, torsions of periodicity 1-3 with barriers
-    0-2 kcal/mol) carrying hydrogens at 1.0-1.09 A; charges N(0, 0.3 e) shifted
-    to the net charge; LJ sigma 2.5-3.5 A, eps 0.02-0.2.  Hydrogens are turned
+    0-2 kcal/mol) carrying hydrogens at 1.0-1.09 A; heavy-atom charges
+    N(0, 0.3 e) shifted to the net charge, hydrogen charges |N(0.1, 0.04)| e
+    (small and positive, so that no H-H pair attracts through the soft H core);
+    LJ sigma 2.5-3.5 A, eps 0.02-0.2 (H: 2.5 A, 0.03).  Hydrogens are turned
     about their heavy atom for the largest clearance, and a geometry is kept
     only if every pair outside the AMBER exclusions (1-2, 1-3, 1-4) is at
-    least 0.8 sigma apart."""
+    least 0.7 sigma apart."""
     n_heavy = max(3, n_atoms // 3)
     n_h = n_atoms - n_heavy
     n_heavy_types = 6
@@ -186,8 +188,8 @@ def chain(n_atoms: int, charge: float, rng: np.random.Generator) -> Species:
     per[: n_h % n_heavy] += 1
     hpar = [i for i in range(n_heavy) for _ in range(per[i])]
     mass = list(rng.choice([12.011, 14.007, 15.999], n_heavy_types)) + [1.008]
-    eps = list(rng.uniform(0.02, 0.2, n_heavy_types)) + [0.02]
-    sigma = list(rng.uniform(2.5, 3.5, n_heavy_types)) + [2.2]
+    eps = list(rng.uniform(0.02, 0.2, n_heavy_types)) + [0.03]
+    sigma = list(rng.uniform(2.5, 3.5, n_heavy_types)) + [2.5]
     types = list(rng.integers(0, n_heavy_types, n_heavy)) + [n_heavy_types] * n_h
     sig = np.array([sigma[t] for t in types])
     n = n_heavy + n_h
@@ -226,7 +228,7 @@ def chain(n_atoms: int, charge: float, rng: np.random.Generator) -> Species:
 
     def clearance_ok(xs):
         d = np.linalg.norm(xs[:, None] - xs[None], axis=2)
-        lim = 0.8 * 0.5 * (sig[:, None] + sig[None, :])
+        lim = 0.7 * 0.5 * (sig[:, None] + sig[None, :])
         bad = d < lim
         for (a, b) in excl:
             bad[a, b] = bad[b, a] = False
@@ -317,8 +319,8 @@ def chain(n_atoms: int, charge: float, rng: np.random.Generator) -> Species:
         dih_rows.append(list(t) + [len(dih_multi)])
         dih_multi.append(1)
         dih_coeff.append(_dih_row([(rng.uniform(0, 0.3), 3, 0.0)]))
-    q = rng.normal(0, 0.3, n)
-    q += (charge - q.sum()) / n
+    q = np.concatenate([rng.normal(0, 0.3, n_heavy), np.abs(rng.normal(0.1, 0.04, n_h))])
+    q[:n_heavy] += (charge - q.sum()) / n_heavy
     xs = xs - xs.mean(axis=0)
     return Species(
         names=[f"X{k}" for k in range(n_heavy_types)] + ["H"],
@@ -361,9 +363,17 @@ def _split_rigid(sp: Species, shake_h: bool):
 def assemble(ion: Species, gas: Species, vap: Species, *, gas_name: str, n_gas: int,
              n_vap: int, T: float, p: float, dt: float, interactions: int, seed: int,
              shake_h: bool, rng: np.random.Generator, nvt_mode=abi.NVT_OFF,
-             min_dist: float = 10.0, box: Optional[float] = None, label: str = "") -> ReplicaSpec:
+             min_dist: float = 10.0, box: Optional[float] = None, label: str = "",
+             reference_masses: bool = False) -> ReplicaSpec:
     """Concatenates the species' tables (ion, gas, vapor order), places the
-    molecules uniformly in the cube and draws Maxwell-Boltzmann velocities."""
+    molecules uniformly in the cube and draws Maxwell-Boltzmann velocities.
+
+    The gas molecule's COM mass is the sum of its atoms' masses, so that the
+    centre-of-mass bookkeeping and the atom masses agree.  reference_masses=True
+    takes the reference's hard-coded molecular mass instead
+    (src/pairList/updateGasIn.cpp, src/initialization/initializationGas.cpp:
+    He 4.027 vs the atom's 4.0026, Ar 28.02 vs 39.948), which puts an argon
+    molecule's COM velocity 30% off its atom's."""
     offs_t, offs_b, offs_a, offs_d = [0], [0], [0], [0]
     mass, eps, sig, names = [], [], [], []
     bc, ac, dm, dc = [], [], [], []
@@ -420,7 +430,8 @@ def assemble(ion: Species, gas: Species, vap: Species, *, gas_name: str, n_gas: 
                 ok[b:b + 4096] &= d >= min_dist
         gx = np.concatenate([gx, c[ok]])[:n_gas]
     g = GAS_TABLE[gas_name]
-    gas_m = mb_mass_kg(g["mol_mass"])
+    gas_com = g["mol_mass"] if reference_masses else float(sum(mass[t] for t in gas_top.type))
+    gas_m = mb_mass_kg(gas_com)
     vap_com = float(sum(mass[t] for t in vap_top.type))
     vap_m = mb_mass_kg(vap_com)
     gv = rng.normal(size=(n_gas, 3)) * mb_sigma(T, gas_m)
@@ -431,7 +442,7 @@ def assemble(ion: Species, gas: Species, vap: Species, *, gas_name: str, n_gas: 
         bond_coeff=np.array(bc).reshape(-1, 2), angle_coeff=np.array(ac).reshape(-1, 2),
         dihedral_multi=np.array(dm, np.int32), dihedral_coeff=np.array(dc).reshape(-1, 15),
         ion=ion_top, ion_v=ion_v, ion_bmh_type=bmh,
-        gas=gas_top, gas_kind=g["kind"], gas_com_mass=g["mol_mass"], gas_mb_mass=gas_m,
+        gas=gas_top, gas_kind=g["kind"], gas_com_mass=gas_com, gas_mb_mass=gas_m,
         vapor=vap_top, vapor_com_mass=vap_com, vapor_mb_mass=vap_m,
         gas_x=gx, gas_v=gv, vapor_x=vx, vapor_v=vv,
         dt=dt, temperature=T, box=box, interactions=interactions, nvt_mode=nvt_mode,

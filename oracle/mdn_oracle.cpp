@@ -382,7 +382,34 @@ struct Oracle {
     for (int m : vap_in) com(1 + n_gas + m, &vx[(size_t)m * a_v], &vv[(size_t)m * a_v], vap, vap_com_mass);
   }
 
-  void insert_gas(int m) {
+  /* Philox word of insertion draw t (word 1 is the N2 spin) */
+  static int insert_word(int t) { return t == 0 ? 0 : 1 + t; }
+
+  /* atoms in the domain before this rebuild: the core (ion + vapor) and the
+   * gas; atoms of vapor molecules whose entry this rebuild accepted */
+  std::vector<V3> core_before, gas_before, new_vapor;
+  int n_vapor_candidates = 0;
+
+  /* no atom of X within MDN_INSERT_MIN_DIST of the core and, for an entering
+   * vapor molecule, of the in-domain gas (for an entering gas molecule, of
+   * the vapor molecules accepted in this rebuild) */
+  bool insert_clear(const V3* X, int n, bool vapor) const {
+    const double d2min = MDN_INSERT_MIN_DIST * MDN_INSERT_MIN_DIST;
+    for (const V3& c : core_before)
+      for (int a = 0; a < n; a++) {
+        double dx = X[a][0] - c[0], dy = X[a][1] - c[1], dz = X[a][2] - c[2];
+        if (dx * dx + dy * dy + dz * dz < d2min) return false;
+      }
+    const std::vector<V3>& extra = vapor ? gas_before : new_vapor;
+    for (const V3& c : extra)
+      for (int a = 0; a < n; a++) {
+        double dx = X[a][0] - c[0], dy = X[a][1] - c[1], dz = X[a][2] - c[2];
+        if (dx * dx + dy * dy + dz * dz < d2min) return false;
+      }
+    return true;
+  }
+
+  void insert_gas(int m, int t = 0) {
     int mi = 1 + m;
     V3* x = &gx[(size_t)m * a_g];
     V3* v = &gv[(size_t)m * a_g];
@@ -397,7 +424,7 @@ struct Oracle {
       v[0] = {0, vy_rot, vz_use};
       v[1] = {0, -vy_rot, -vz_use};
     }
-    orc::U4 s = draw(mi, 1, 0);
+    orc::U4 s = draw(mi, 1, insert_word(t));
     double a = orc::u01(s.v[0]) * 2 * M_PI;
     double b = orc::u01(s.v[1]) * 2 * M_PI;
     double c = orc::u01(s.v[2]) * 2 * M_PI;
@@ -419,7 +446,7 @@ struct Oracle {
     for (int k = 0; k < a_g; k++) gf[(size_t)m * a_g + k] = {0, 0, 0};
   }
 
-  void insert_vapor(int m) {
+  void insert_vapor(int m, int t = 0) {
     int mi = 1 + n_gas + m;
     V3* x = &vx[(size_t)m * a_v];
     V3* v = &vv[(size_t)m * a_v];
@@ -431,7 +458,7 @@ struct Oracle {
      * of its previous visit, which this restatement (and the engine) also
      * sets to 0 */
     for (int a = 0; a < a_v; a++) vw[(size_t)m * a_v + a] = 0;
-    orc::U4 s = draw(mi, 1, 0);
+    orc::U4 s = draw(mi, 1, insert_word(t));
     double a = orc::u01(s.v[0]) * 2 * M_PI;
     double b = orc::u01(s.v[1]) * 2 * M_PI;
     double c = orc::u01(s.v[2]) * 2 * M_PI;
@@ -471,10 +498,32 @@ struct Oracle {
       double dz = x[2] - x0[2];
       double r2 = (dx * dx + dy * dy + dz * dz);
       if (r2 < RI2) {
-        in_list.push_back(q);
         if (!region[i]) {
-          if (vapor) insert_vapor(q); else insert_gas(q);
+          if (quirks & MDN_Q_BLIND_INSERT) {
+            if (vapor) insert_vapor(q); else insert_gas(q);
+          } else {
+            /* re-draw the rotation until no atom overlaps; all draws failing
+             * leaves the molecule outside until the next rebuild; at most 64
+             * vapor entries are tested per rebuild, later ones wait */
+            if (vapor && n_vapor_candidates++ >= 64) {
+              region[i] = 0;
+              continue;
+            }
+            int t = 0;
+            for (; t < MDN_INSERT_TRIES; t++) {
+              if (vapor) insert_vapor(q, t); else insert_gas(q, t);
+              const V3* X = vapor ? &vx[(size_t)q * a_v] : &gx[(size_t)q * a_g];
+              if (insert_clear(X, vapor ? a_v : a_g, vapor)) break;
+            }
+            if (t == MDN_INSERT_TRIES) {
+              region[i] = 0;
+              continue;
+            }
+            if (vapor)
+              for (int a = 0; a < a_v; a++) new_vapor.push_back(vx[(size_t)q * a_v + a]);
+          }
         }
+        in_list.push_back(q);
         region[i] = 1;
       } else {
         region[i] = 0;
@@ -526,8 +575,19 @@ struct Oracle {
       for (int k = 0; k < 3; k++) mol_x[i][k] += mol_v[i][k] * dt * loop_pair;
     }
     update_in_centers();
-    classify(1, n_gas, gas_in, false);
+    core_before.assign(ion_x.begin(), ion_x.end());
+    for (int q : vap_in)
+      for (int a = 0; a < a_v; a++) core_before.push_back(vx[(size_t)q * a_v + a]);
+    gas_before.clear();
+    if (!(quirks & MDN_Q_BLIND_INSERT))
+      for (int m : gas_in)
+        for (int a = 0; a < a_g; a++) gas_before.push_back(gx[(size_t)m * a_g + a]);
+    /* vapor entries are decided first so that gas entries are tested against
+     * them (each molecule's draws are independent of this order) */
+    new_vapor.clear();
+    n_vapor_candidates = 0;
     classify(1 + n_gas, n_vap, vap_in, true);
+    classify(1, n_gas, gas_in, false);
     make_lists();
     double vmax2 = 0.0;
     for (auto& v : mol_v) {

@@ -21,6 +21,10 @@ from tests.gpu_helpers import compare_states, force_ok, forces_of, need_gpu, rel
 pytestmark = pytest.mark.gpu
 
 NAMES = list(systems.ALL)
+# the reference's insertion (one random rotation, no overlap test) and the
+# checked insertion (rotation re-drawn until nothing lies within 2 A)
+CHECKED = abi.Q_ALL & ~abi.Q_BLIND_INSERT
+INSERTION = [pytest.param(abi.Q_ALL, id="blind"), pytest.param(CHECKED, id="checked")]
 
 
 @pytest.fixture(scope="module")
@@ -28,11 +32,12 @@ def eng():
     return need_gpu()
 
 
+@pytest.mark.parametrize("quirks", INSERTION)
 @pytest.mark.parametrize("name", NAMES)
-def test_initial_make_pair_matches_oracle(eng, oracle_libs, name):
+def test_initial_make_pair_matches_oracle(eng, oracle_libs, name, quirks):
     spec = systems.make(name)
-    e = eng.Engine([spec])
-    o = oracle_libs.OracleReplica(spec)
+    e = eng.Engine([spec], quirks=quirks)
+    o = oracle_libs.OracleReplica(spec, quirks=quirks)
     a, b = e.state(0), o.get_state()
     i = e.info(0)
     assert i.status == 0
@@ -71,15 +76,16 @@ def test_forces_match_fp64_oracle(eng, oracle_libs, name, term):
     assert np.all(np.abs(Ue - Uo) <= 1e-4 * scale + 1e-6), f"energies {Ue} vs {Uo}"
 
 
+@pytest.mark.parametrize("quirks", INSERTION)
 @pytest.mark.parametrize("name", NAMES)
-def test_trajectory_across_rebuild(eng, oracle_libs, name):
+def test_trajectory_across_rebuild(eng, oracle_libs, name, quirks):
     """30 steps with a rebuild at the first step (loop_pair = loop_update)."""
     spec = systems.make(name)
-    o = oracle_libs.OracleReplica(spec)
+    o = oracle_libs.OracleReplica(spec, quirks=quirks)
     o.step(2)
     st = o.get_state()
     st.loop_pair, st.loop_update = 5, 5
-    e = eng.Engine([spec])
+    e = eng.Engine([spec], quirks=quirks)
     e.upload(0, st)
     o.set_state(st)
     e.step(30, energy_mode=1)
@@ -91,6 +97,25 @@ def test_trajectory_across_rebuild(eng, oracle_libs, name):
     assert err <= 1e-4
     Ue, Uo = e.energies()[0], o.energies()
     assert np.all(np.abs(Ue - Uo) <= 1e-4 * max(np.abs(Uo).max(), 1e-3) + 1e-6)
+
+
+def test_dense_batched_replica_tracks_oracle(eng, oracle_libs):
+    """A replica of the 256-replica batch workload at full density (about
+    14,000 gas molecules in the domain), four blocks of 100 steps with the
+    checked insertion: the rebuild count and the in-domain sets agree, and
+    positions stay within 1e-4 A (the trajectory is chaotic; FP32 pair sums
+    separate it from the FP64 oracle by ~1e-9 A per step at first)."""
+    from md_nucleation_b200 import generate
+    spec = generate.config2_replica(2)
+    e = eng.Engine([spec], quirks=CHECKED)
+    o = oracle_libs.OracleReplica(spec, quirks=CHECKED)
+    for _ in range(4):
+        e.step(100)
+        o.step(100)
+        assert e.status()[0] == 0
+        assert e.info(0).n_rebuilds == o.info().n_rebuilds
+    assert e.info(0).n_rebuilds >= 2
+    compare_states(e.state(0), o.get_state(), spec, xtol=1e-4, vtol=1e-5, what="config2 replica 2")
 
 
 def test_shake_constraints_hold(eng):
