@@ -202,18 +202,10 @@ class stdout_to_stderr:
         os.close(self.saved)
 
 
-def cpu_sample(specs, threads: int, budget_s: float):
-    """Times the reference's MD::verlet (SHAKE step where the replica has
-    SHAKE) on `2 * threads` replicas spread over the batch, one replica per
-    OpenMP thread at a time (src/main.cpp:22-29); returns (atom-steps/s, what
-    was sampled).  The step count is sized from a 5-step calibration so the
-    sample takes about `budget_s`."""
+def _cpu_sample_child(specs, threads, budget_s, q):
     from oracle import bind
-    stride = max(1, len(specs) // (2 * threads))
-    pick = list(range(0, len(specs), stride))[:2 * threads]
     with stdout_to_stderr():
-        reps = [bind.RefReplica(specs[r]) for r in pick]
-    atoms = sum(r.in_domain_atoms() for r in reps)
+        reps = [bind.RefReplica(sp) for sp in specs]
     t0 = time.perf_counter()
     bind.ref_verlet_many(reps, 5, threads)
     cal = (time.perf_counter() - t0) / 5
@@ -223,10 +215,35 @@ def cpu_sample(specs, threads: int, budget_s: float):
     bind.ref_verlet_many(reps, n, threads)
     dt = time.perf_counter() - t0
     atoms1 = sum(r.in_domain_atoms() for r in reps)
-    value = 0.5 * (atoms0 + atoms1) * n / dt
-    sample = (f"{len(reps)} of the {len(specs)} replicas (every {stride}th), {n} MD steps each, "
-              f"{atoms} in-domain atoms at the start, {dt:.1f} s wall")
-    return value, sample, len(reps), n, dt
+    q.put((0.5 * (atoms0 + atoms1) * n / dt, n, atoms0, dt))
+
+
+def cpu_sample(specs, threads: int, budget_s: float):
+    """Times the reference's MD::verlet on `2 * threads` replicas spread over
+    the batch, one replica per OpenMP thread at a time (src/main.cpp:22-29);
+    returns (atom-steps/s, what was sampled), or (None, reason).  The step
+    count is sized from a 5-step calibration so the sample takes about
+    `budget_s`; the sample runs in a child process that is ended after
+    3 * budget_s + 120 s."""
+    ctx = mp.get_context("spawn")
+    stride = max(1, len(specs) // (2 * threads))
+    pick = [specs[r] for r in list(range(0, len(specs), stride))[:2 * threads]]
+    q = ctx.Queue()
+    p = ctx.Process(target=_cpu_sample_child, args=(pick, threads, budget_s, q))
+    p.start()
+    limit = 3 * budget_s + 120
+    try:
+        value, n, atoms, dt = q.get(timeout=limit)
+        sample = (f"{len(pick)} of the {len(specs)} replicas (every {stride}th), {n} MD steps each "
+                  f"(MD::verlet as shipped: X-H bonds unconstrained, no SHAKE), {atoms} in-domain "
+                  f"atoms, {dt:.1f} s wall on {threads} threads")
+    except Exception:
+        value, sample = None, f"the reference sample did not finish within {limit:.0f} s"
+    p.join(timeout=10)
+    if p.is_alive():
+        p.kill()
+        p.join()
+    return value, sample
 
 
 def host_threads():
@@ -249,7 +266,10 @@ def run_reference(args):
     values = []
     sample = ""
     for k in range(args.warmup + args.steps):
-        v, sample, nrep, n, dt = cpu_sample(specs, threads, args.ref_budget)
+        v, sample = cpu_sample(specs, threads, args.ref_budget)
+        if v is None:
+            print(json.dumps({"impl": "reference", "unavailable": sample}))
+            return 0
         if k >= args.warmup:
             values.append(v)
         log(f"reference step {k}: {v:.4g} atom-steps/s ({sample})")
@@ -397,7 +417,7 @@ def run_engine(args):
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         from oracle import bind
         if bind.have_reference():
-            v, sample, nrep, n, dt = cpu_sample(specs, threads, args.cpu_budget)
+            v, sample = cpu_sample(specs, threads, args.cpu_budget)
             out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
                                    "sample": sample}
         else:

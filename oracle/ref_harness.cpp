@@ -58,7 +58,6 @@ namespace {
 struct Harness {
   MD* md;
   int n_ion, a_g, a_v, n_gas, n_vap;
-  bool shake = false;     /* the replica's X-H bonds are SHAKE constraints */
   std::vector<int> perm;  /* descriptor type -> reference type row */
 };
 
@@ -94,7 +93,6 @@ void* ref_create(const mdn_replica_desc* d, int do_make_pair) {
   h->a_v = d->vapor.n_atoms;
   h->n_gas = d->n_gas;
   h->n_vap = d->n_vapor;
-  h->shake = (d->interactions & MDN_I_SHAKE) != 0;
 
   /* run parameters (src/initialization/setCondition.cpp:119-146,247-250) */
   md->dt = d->dt;
@@ -610,18 +608,16 @@ void ref_export_dump(void* hp, const char* path, double time_fs) {
 
 extern "C" {
 /* The reference's replica model (src/main.cpp:22-29): one replica per OpenMP
- * thread, each running MD::verlet n times (the SHAKE step of ref_verlet_shake
- * when the replica constrains its X-H bonds).  threads <= 0: all threads. */
+ * thread, each running MD::verlet n times.  threads <= 0: all threads.
+ * MD::verlet never calls the reference's SHAKE (src/verlet.cpp:24); its
+ * iteration has no iteration limit, so it is not run here on replicas that
+ * the reference's insertion may have blown up. */
 void ref_verlet_many(void** hs, int n, long long steps, int threads) {
   if (threads > 0) omp_set_num_threads(threads);
 #pragma omp parallel for schedule(dynamic, 1)
   for (int i = 0; i < n; i++) {
-    Harness* h = (Harness*)hs[i];
-    if (h->shake) {
-      ref_verlet_shake(h, steps, 0, nullptr);
-      continue;
-    }
-    for (long long s = 0; s < steps; s++) h->md->verlet();
+    MD* md = ((Harness*)hs[i])->md;
+    for (long long s = 0; s < steps; s++) md->verlet();
   }
 }
 }

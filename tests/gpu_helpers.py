@@ -43,7 +43,12 @@ def force_ok(a, b):
 
 def compare_states(a, b, spec, xtol, vtol, what=""):
     """Positions and velocities of every in-domain atom and molecule centre."""
-    assert np.array_equal(a.region, b.region), f"{what}: region flags differ"
+    if not np.array_equal(a.region, b.region):
+        bad = np.nonzero(a.region != b.region)[0]
+        c = b.mol_x[0]
+        desc = [f"mol {m}: engine {a.region[m]} oracle {b.region[m]} "
+                f"r/R_I {np.linalg.norm(b.mol_x[m] - c) / spec.r_inter:.9f}" for m in bad[:6]]
+        raise AssertionError(f"{what}: region flags differ for {len(bad)} molecules: " + "; ".join(desc))
     g, v = in_masks(a, spec)
     checks = [("ion_x", a.ion_x, b.ion_x, xtol), ("ion_v", a.ion_v, b.ion_v, vtol),
               ("gas_x", a.gas_ax[g], b.gas_ax[g], xtol), ("gas_v", a.gas_av[g], b.gas_av[g], vtol),
