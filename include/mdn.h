@@ -98,6 +98,8 @@ extern "C" {
                                      position-only form heats the system */
 #define MDN_INSERT_MIN_DIST 2.0  /* A, the overlap test of the checked insertion */
 #define MDN_INSERT_TRIES    4
+#define MDN_INSERT_MAX_VAPOR 256 /* vapor entries tested per rebuild; later ones wait
+                                    for the next rebuild */
 
 /* energy buckets, the order of `struct Potentials` (src/struct.hpp:29-38) */
 #define MDN_U_ION 0

@@ -74,7 +74,7 @@ struct Ctx {
   int n_core;       /* atoms in the core                */
   int buf;          /* which acc buffer holds this step */
   int* iscr;        /* >= 64 ints of scratch            */
-  int* cand;        /* [65] entering vapor molecules    */
+  int* cand;        /* [MDN_INSERT_MAX_VAPOR + 1] entering vapor molecules, count last */
   double* trial;    /* [3*MDN_MAX_VAP_ATOMS] trial atoms */
   double* dscr;     /* >= 64 doubles of scratch         */
   const int* ib;    /* int blob of the replica          */
@@ -907,8 +907,11 @@ __device__ void gas_far_pass(Ctx& x, bool eflag, bool kick) {
   }
 }
 
-/* near molecules: one warp each; gas-ion and gas-vapor lists; the molecule's
- * own force is reduced over the warp, the reaction goes to the core sums */
+/* near molecules (those with a gas-ion or gas-vapor list entry): one thread
+ * each, walking the molecule's lists (about one entry per molecule in the
+ * batched workload, so a wider split leaves lanes idle); the molecule's own
+ * force stays in registers, the reaction goes to the core sums by shared
+ * 64-bit integer atomics, so the result does not depend on the order */
 __device__ void gas_near_pass(Ctx& x, bool eflag, bool kick) {
   const RepParams* P = x.P;
   const KArgs* a = x.a;
@@ -916,7 +919,6 @@ __device__ void gas_near_pass(Ctx& x, bool eflag, bool kick) {
   const bool gi = term_on(x, MDN_I_GI), gv = term_on(x, MDN_I_GV);
   const bool intra = term_on(x, MDN_I_GAS_INTRA) && P->n_gas_bonds > 0;
   const int nj = (P->quirks & MDN_Q_GV_GAS_COUNT) ? min(ag, av) : av;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   int lo, hi;
   partition(x, x.D->n_gas_in, &lo, &hi);
   /* this CTA's range of the (ascending) near list */
@@ -939,7 +941,7 @@ __device__ void gas_near_pass(Ctx& x, bool eflag, bool kick) {
   }
   const double* com = x.D->ion_com;
   long long egi = 0, egv = 0, eintra = 0;
-  for (int e = b0 + wid; e < b1; e += nw) {
+  for (int e = b0 + (int)threadIdx.x; e < b1; e += blockDim.x) {
     const int s = nl[e];
     const size_t ms = gmol(P, par, s);
     float3 gp[MDN_MAX_GAS_ATOMS];
@@ -954,7 +956,7 @@ __device__ void gas_near_pass(Ctx& x, bool eflag, bool kick) {
     for (int at = 0; at < MDN_MAX_GAS_ATOMS; at++) F[at][0] = F[at][1] = F[at][2] = 0;
     if (gi) {
       const int start = a->near_gi[ms], cnt = a->gil_n[ms];
-      for (int q = lane; q < cnt; q += 32) {
+      for (int q = 0; q < cnt; q++) {
         int j = a->gil[P->gil_off + start + q];
         float4 pj = x.c.pos[j];
         int tj = x.c.type[j];
@@ -976,55 +978,52 @@ __device__ void gas_near_pass(Ctx& x, bool eflag, bool kick) {
     }
     if (gv) {
       const int start = a->near_gv[ms], cnt = a->gvl_n[ms];
-      const int tot = cnt * nj;
-      for (int q = lane; q < tot; q += 32) {
-        int ent = q / nj, b = q - ent * nj;
-        int vs = a->gvl[P->gvl_off + start + ent];
-        int j = ni + vs * av + b;
-        float4 pj = x.c.pos[j];
-        int tj = x.c.type[j];
-        long long R[3] = {0, 0, 0};
-        for (int at = 0; at < ag; at++) {
-          float dx = gp[at].x - pj.x, dy = gp[at].y - pj.y, dz = gp[at].z - pj.z;
-          float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-          float ee;
-          float fp = lj_coul(r2, x.c.ljA[gtype[at] * nt + tj], x.c.ljB[gtype[at] * nt + tj], 0.0f, false, &ee);
-          long long fx = fixf(fp * dx), fy = fixf(fp * dy), fz = fixf(fp * dz);
-          F[at][0] += fx; F[at][1] += fy; F[at][2] += fz;
-          R[0] -= fx; R[1] -= fy; R[2] -= fz;
-          if (eflag)
-            egv += efixd(lj_coul_energy(r2d(X + 3 * at, x.c.x + 3 * j), x.db[P->d_ljA + gtype[at] * nt + tj],
-                                        x.db[P->d_ljB + gtype[at] * nt + tj], 0.0));
+      for (int ent = 0; ent < cnt; ent++) {
+        const int vs = a->gvl[P->gvl_off + start + ent];
+        for (int b = 0; b < nj; b++) {
+          int j = ni + vs * av + b;
+          float4 pj = x.c.pos[j];
+          int tj = x.c.type[j];
+          long long R[3] = {0, 0, 0};
+          for (int at = 0; at < ag; at++) {
+            float dx = gp[at].x - pj.x, dy = gp[at].y - pj.y, dz = gp[at].z - pj.z;
+            float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            float ee;
+            float fp = lj_coul(r2, x.c.ljA[gtype[at] * nt + tj], x.c.ljB[gtype[at] * nt + tj], 0.0f, false, &ee);
+            long long fx = fixf(fp * dx), fy = fixf(fp * dy), fz = fixf(fp * dz);
+            F[at][0] += fx; F[at][1] += fy; F[at][2] += fz;
+            R[0] -= fx; R[1] -= fy; R[2] -= fz;
+            if (eflag)
+              egv += efixd(lj_coul_energy(r2d(X + 3 * at, x.c.x + 3 * j), x.db[P->d_ljA + gtype[at] * nt + tj],
+                                          x.db[P->d_ljB + gtype[at] * nt + tj], 0.0));
+          }
+          acc_add(x, j, R);
         }
-        acc_add(x, j, R);
       }
     }
+    double Fd[3 * MDN_MAX_GAS_ATOMS];
     for (int at = 0; at < ag; at++)
-      for (int k = 0; k < 3; k++) F[at][k] = warp_sum_ll(F[at][k]);
-    if (lane == 0) {
-      double Fd[3 * MDN_MAX_GAS_ATOMS];
-      for (int at = 0; at < ag; at++)
-        for (int k = 0; k < 3; k++) {
-          Fd[3 * at + k] = (double)F[at][k] * MDN_FIX_INV;
-          if (!(fabs(Fd[3 * at + k]) < MDN_FIX_LIMIT)) set_status(x, MDN_ST_FIXED_OVERFLOW);
-        }
-      if (intra) {
-        double ei = gas_intra(x, X, Fd);
-        if (eflag) eintra += efixd(ei);
+      for (int k = 0; k < 3; k++) {
+        Fd[3 * at + k] = (double)F[at][k] * MDN_FIX_INV;
+        if (!(fabs(Fd[3 * at + k]) < MDN_FIX_LIMIT)) set_status(x, MDN_ST_FIXED_OVERFLOW);
       }
-      for (int at = 0; at < ag; at++) {
-        size_t g = gatom(P, par, s, at);
-        for (int k = 0; k < 3; k++) {
-          if (kick) a->slab_v[3 * g + k] += Fd[3 * at + k] * c2[at];
-          a->slab_f[3 * g + k] = Fd[3 * at + k];
-        }
+    if (intra) {
+      double ei = gas_intra(x, X, Fd);
+      if (eflag) eintra += efixd(ei);
+    }
+    for (int at = 0; at < ag; at++) {
+      size_t g = gatom(P, par, s, at);
+      for (int k = 0; k < 3; k++) {
+        if (kick) a->slab_v[3 * g + k] += Fd[3 * at + k] * c2[at];
+        a->slab_f[3 * g + k] = Fd[3 * at + k];
       }
     }
   }
   if (eflag) {
     egi = warp_sum_ll(egi);
     egv = warp_sum_ll(egv);
-    if (lane == 0) {
+    eintra = warp_sum_ll(eintra);
+    if ((threadIdx.x & 31) == 0) {
       energy_add(x, MDN_U_GI, egi);
       energy_add(x, MDN_U_VG, egv);
       energy_add(x, MDN_U_GAS, eintra);
@@ -1109,7 +1108,7 @@ __device__ bool insert_clear(const Ctx& x, const double* X, int n, int n_rebuild
       if (dx * dx + dy * dy + dz * dz < d2min) return false;
     }
   }
-  const int nc = min(x.cand[64], 64);
+  const int nc = min(x.cand[MDN_INSERT_MAX_VAPOR], MDN_INSERT_MAX_VAPOR);
   for (int k = 0; k < nc; k++) {
     const int mi = x.cand[k];
     const int f = x.a->region[(size_t)x.P->mol_off + mi];
@@ -1206,9 +1205,10 @@ __device__ __forceinline__ int classify_one(const Ctx& x, int mi, double sigma, 
   int draw_ok = 0;
   if (in && !was && !(P->quirks & MDN_Q_BLIND_INSERT) && kind == 1) {
     /* decided by vapor_entries(): recorded as a candidate, provisionally in;
-     * beyond 64 candidates in one rebuild the entry waits for the next */
-    int c = atomicAdd(&x.cand[64], 1);
-    if (c >= 64) {
+     * beyond MDN_INSERT_MAX_VAPOR candidates in one rebuild the entry waits
+     * for the next */
+    int c = atomicAdd(&x.cand[MDN_INSERT_MAX_VAPOR], 1);
+    if (c >= MDN_INSERT_MAX_VAPOR) {
       x.a->region[g] = 0;
       return 0;
     }
@@ -1391,7 +1391,7 @@ __device__ int vapor_entries(Ctx& x, int nreb) {
   const KArgs* a = x.a;
   const int av = P->a_v, ag = P->a_g, par = x.D->parity, G = x.D->n_gas_in;
   const double d2min = MDN_INSERT_MIN_DIST * MDN_INSERT_MIN_DIST;
-  const int nc = min(x.cand[64], 64);
+  const int nc = min(x.cand[MDN_INSERT_MAX_VAPOR], MDN_INSERT_MAX_VAPOR);
   int deferred = 0;
   for (int c = 0; c < nc; c++) {
     const int mi = x.cand[c];
@@ -1510,7 +1510,7 @@ __device__ void make_pair(Ctx& x, cg::cluster_group& cl) {
   double vmax2 = 0;
   /* vapor molecules (rank 0; events) */
   int my_vin = 0;
-  if (threadIdx.x == 0) x.cand[64] = 0;
+  if (threadIdx.x == 0) x.cand[MDN_INSERT_MAX_VAPOR] = 0;
   __syncthreads();
   if (x.rank == 0)
     for (int q = threadIdx.x; q < P->n_vap; q += blockDim.x) {
@@ -1550,7 +1550,7 @@ __device__ void make_pair(Ctx& x, cg::cluster_group& cl) {
   __threadfence();
   cl.sync();
   if (x.rank != 0) {
-    for (int k = threadIdx.x; k <= 64; k += blockDim.x) x.cand[k] = *cl.map_shared_rank(&x.cand[k], 0);
+    for (int k = threadIdx.x; k <= MDN_INSERT_MAX_VAPOR; k += blockDim.x) x.cand[k] = *cl.map_shared_rank(&x.cand[k], 0);
   }
   __syncthreads();
   /* free flight + classification of the gas molecules of this CTA's range */
@@ -1751,7 +1751,7 @@ extern "C" __global__ void __launch_bounds__(512, 1) mdn_advance(KArgs a) {
   __shared__ int s_job;
   __shared__ int iscr[64];
   __shared__ double dscr[64];
-  __shared__ int cand[65];
+  __shared__ int cand[MDN_INSERT_MAX_VAPOR + 1];
   __shared__ double trial[3 * MDN_MAX_VAP_ATOMS];
 
   Ctx x;

@@ -503,9 +503,9 @@ struct Oracle {
             if (vapor) insert_vapor(q); else insert_gas(q);
           } else {
             /* re-draw the rotation until no atom overlaps; all draws failing
-             * leaves the molecule outside until the next rebuild; at most 64
+             * leaves the molecule outside until the next rebuild; at most MDN_INSERT_MAX_VAPOR
              * vapor entries are tested per rebuild, later ones wait */
-            if (vapor && n_vapor_candidates++ >= 64) {
+            if (vapor && n_vapor_candidates++ >= MDN_INSERT_MAX_VAPOR) {
               region[i] = 0;
               continue;
             }

@@ -103,8 +103,8 @@ def test_dense_batched_replica_tracks_oracle(eng, oracle_libs):
     """A replica of the 256-replica batch workload at full density (about
     14,000 gas molecules in the domain) with the checked insertion: four
     blocks of 100 steps, each started from the oracle's state (a free-running
-    comparison separates chaotically, FP32 pair sums against FP64), crossing
-    rebuilds; the rebuild count and the in-domain sets agree and positions
+    comparison separates chaotically, FP32 pair sums against FP64), blocks 1
+    and 3 with a rebuild at their first step; the rebuild count and the in-domain sets agree and positions
     stay within 1e-5 A, velocities within 1e-6 A/fs (in this 5.5e6 Pa helium
     the FP32 rounding of the pair forces grows to ~1.5e-6 A within one block)."""
     from md_nucleation_b200 import generate
@@ -114,7 +114,11 @@ def test_dense_batched_replica_tracks_oracle(eng, oracle_libs):
     rebuilds = 0
     for block in range(4):
         assert e.info(0).n_rebuilds == o.info().n_rebuilds
-        e.upload(0, o.get_state())
+        st = o.get_state()
+        if block % 2:  # a rebuild at the block's first step
+            st.loop_pair, st.loop_update = 5, 5
+            o.set_state(st)
+        e.upload(0, st)
         r0 = o.info().n_rebuilds
         e.step(100)
         o.step(100)
