@@ -286,6 +286,29 @@ int  mdn_in_domain(mdn_handle* h, int replica, int capacity, int* count,
  * MDN_ERR_CAPACITY, with offset filled, when capacity is too small.        */
 int  mdn_snapshot(mdn_handle* h, long long* offset, long long capacity, int* type, double* x, double* v,
                   double* U);
+/* mdn_snapshot without any device allocation.  No counterpart in the
+ * reference (its dump loop reads host memory).  mdn_snapshot allocates its
+ * device staging on its first call, sized for every replica's largest
+ * possible domain (hundreds of MB for a large batch).  A program that has
+ * handed all free device memory to its own pool, or that runs under a fixed
+ * device-memory budget, cannot let a dump taken late in a run allocate, or
+ * fail for lack of memory.  This call stages the rows in a fixed array that
+ * the library holds on each device from the moment it is loaded there:
+ * MDN_NOALLOC_MAX_ROWS rows (52 bytes each) and MDN_NOALLOC_MAX_REPLICAS
+ * replicas, 3.4 MB in all.  A larger snapshot, or a larger batch, returns
+ * MDN_ERR_CAPACITY and says so in mdn_last_error (offset filled when the
+ * replica count fits); use mdn_snapshot for those.  The first call on a
+ * device looks the array up on that device (once per device per process);
+ * make that first call before any stream capture.  Every call in the process
+ * shares the one array per device: calls that overlap in time on the same
+ * device, from different threads or handles, race and may return each
+ * other's rows.  Nothing in the array has to start at zero: each call writes
+ * every offset and every row it copies back.  Arguments and results as
+ * mdn_snapshot. */
+#define MDN_NOALLOC_MAX_ROWS     65536
+#define MDN_NOALLOC_MAX_REPLICAS 1024
+int  mdn_snapshot_noalloc(mdn_handle* h, long long* offset, long long capacity, int* type, double* x,
+                          double* v, double* U);
 /* Page-locked host memory for mdn_snapshot / mdn_upload_state buffers. */
 int  mdn_host_alloc(size_t bytes, void** ptr);
 int  mdn_host_free(void* ptr);

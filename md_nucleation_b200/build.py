@@ -14,7 +14,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libmdn.so")
-SOURCES = ["advance.cu", "snapshot.cu", "engine.cu"]
+SOURCES = ["advance.cu", "snapshot.cu", "snapshot_noalloc.cu", "engine.cu"]
 HEADERS = ["mdn_types.h", "device_util.cuh"]
 
 NVCC_FLAGS = [

@@ -276,6 +276,26 @@ int sync_check(mdn_handle* h) {
 
 }  // namespace
 
+/* Internal, for snapshot_noalloc.cu: the snapshot kernels' inputs of a
+ * handle, and the text mdn_last_error returns. */
+__attribute__((visibility("hidden"))) void mdn_snapshot_args(const mdn_handle* h, SnapshotArgs* s) {
+  s->P = h->dP;
+  s->D = h->dD;
+  s->iblob = h->d_iblob;
+  s->R = h->R;
+  s->dev = h->dev;
+  s->ion_x = h->ion_x;
+  s->ion_v = h->ion_v;
+  s->slab_x = h->slab_x;
+  s->slab_v = h->slab_v;
+  s->vslab_x = h->vslab_x;
+  s->vslab_v = h->vslab_v;
+  s->energy = h->energy;
+  s->stream = (void*)h->stream;
+}
+
+__attribute__((visibility("hidden"))) int mdn_error(int code, const char* msg) { return fail(code, "%s", msg); }
+
 extern "C" {
 
 int mdn_abi_version(void) { return MDN_ABI_VERSION; }

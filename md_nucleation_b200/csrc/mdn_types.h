@@ -144,4 +144,17 @@ typedef struct KArgs {
   int colors_cap;
 } KArgs;
 
+/* A handle's device arrays that the snapshot kernels read (filled by
+ * engine.cu for the allocation-free snapshot); stream is a cudaStream_t. */
+typedef struct {
+  const RepParams* P;
+  const RepDyn* D;
+  const int* iblob;
+  int R;
+  int dev;
+  const double *ion_x, *ion_v, *slab_x, *slab_v, *vslab_x, *vslab_v;
+  const long long* energy;
+  void* stream;
+} SnapshotArgs;
+
 #endif
