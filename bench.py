@@ -246,6 +246,29 @@ def cpu_sample(specs, threads: int, budget_s: float):
     return value, sample
 
 
+def plain_sample(engine, specs, quirks, n_pick: int):
+    """The plain GPU path: each sampled replica alone in its own engine, one
+    kernel launch per MD step (the cluster size is then automatic: 8 CTAs on
+    the one replica).  The replicas run one after another, so the aggregate
+    is their atom-steps over the summed device time."""
+    stride = max(1, len(specs) // n_pick)
+    picks = list(range(0, len(specs), stride))[:n_pick]
+    atom_steps, seconds = 0.0, 0.0
+    for r in picks:
+        e = engine.Engine([specs[r]], quirks=quirks, steps_per_launch=1)
+        e.step(10)
+        a0 = in_domain_atoms([e.info(0)], [specs[r]])[0]
+        e.step(MD_STEPS)
+        ms, _ = e.last_timing()
+        a1 = in_domain_atoms([e.info(0)], [specs[r]])[0]
+        atom_steps += 0.5 * (a0 + a1) * MD_STEPS
+        seconds += ms * 1e-3
+        e.close()
+    sample = (f"{len(picks)} of the {len(specs)} replicas (every {stride}th), each alone, "
+              f"{MD_STEPS} MD steps at one launch per step, {seconds:.2f} s of device time")
+    return atom_steps / seconds, sample
+
+
 def host_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -318,6 +341,10 @@ def run_engine(args):
             dist.barrier()
         torch.cuda.synchronize(device)
 
+    # warm-up: the launch-shape tuner (4 blocks of MD_STEPS, one per cluster
+    # size; results do not depend on the shape), then the warm-up steps
+    tuned = eng.tune_launch(MD_STEPS)
+    log(f"rank {rank}: tuned cluster size {tuned}")
     for _ in range(args.warmup):
         eng.step(MD_STEPS)
     barrier()
@@ -375,6 +402,7 @@ def run_engine(args):
     e2e_all = sum_over_ranks(dist, e2e_atom_steps, device)
     e2e_value = e2e_all / e2e_s
     h2d_per_step = eng.n * (4 + 8)
+    launch_shape = eng.get_launch()
 
     out = None
     if rank == 0:
@@ -391,6 +419,9 @@ def run_engine(args):
                 "l2": f"inputs larger than L2: {resident / 2**30:.2f} GiB resident per GPU",
                 "replicas_with_warnings": warned, "replicas_failed": fatal,
                 "parallelism": f"replicas sharded over {ws} GPU(s), no collective in the step",
+                "launch": {"cluster_ctas_per_replica": launch_shape[0], "threads_per_cta": launch_shape[1],
+                           "md_steps_per_launch": MD_STEPS if launch_shape[2] <= 0 else launch_shape[2],
+                           "chosen_by": "mdn_tune_launch during warm-up"},
             },
             "roofline": {
                 "bound": "fp32", "achieved": achieved_tflops,
@@ -413,6 +444,10 @@ def run_engine(args):
         out["roofline"]["frac"] = achieved_tflops / peak
         out["roofline"]["peak_source"] = (f"{props.multi_processor_count} SMs x 128 FP32 lanes x 2 "
                                           f"at the measured {mhz:.0f} MHz")
+    # the plain one-system-per-launch path on the same GPU (rank 0, N = 1)
+    if rank == 0 and ws == 1 and not args.no_plain:
+        pv, psample = plain_sample(engine, specs, checked, args.plain_replicas)
+        out["plain"] = {"value": pv, "unit": UNIT, "sample": psample, "batched_over_plain": value / pv}
     # CPU baseline on rank 0 at N = 1 only
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         from oracle import bind
@@ -441,6 +476,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of the CPU-baseline sample")
     ap.add_argument("--ref-budget", type=float, default=10.0, help="seconds per reference-arm step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the one-system-per-launch measurement")
+    ap.add_argument("--plain-replicas", type=int, default=16)
     args = ap.parse_args()
     if args.warmup < 3 and not os.environ.get("MDN_BENCH_ALLOW_SHORT"):
         raise SystemExit("bench.py: --warmup must be >= 3")

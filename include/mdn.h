@@ -181,9 +181,10 @@ typedef struct mdn_options {
   int force_mode;            /* 0: FP32 pair math, int64 fixed-point sums (default);
                                 1: FP64 pair math, int64 fixed-point sums            */
   int cluster_size;          /* CTAs cooperating on one replica (1..8); 0 = automatic   */
-  int threads;               /* threads per CTA (128..1024, multiple of 32); 0 = 512    */
+  int threads;               /* threads per CTA (32..512, multiple of 32); 0 = 512      */
   int steps_per_launch;      /* steps advanced per kernel launch; 0 = whole mdn_step    */
-  int use_graph;             /* capture repeated launches in a CUDA graph               */
+  int use_graph;             /* ignored: one launch already advances every step of an
+                                mdn_step call                                          */
   double capacity_factor;    /* slab / list headroom over the expected counts (>= 1)   */
   int device;                /* CUDA device ordinal                                     */
 } mdn_options;
@@ -245,11 +246,14 @@ void mdn_destroy(mdn_handle* h);
  * energy_mode: 0 = no energies, 1 = energies of the last step (eflag on the
  * last step, as MD::run sets it), 2 = energies summed over every step.   */
 int  mdn_step(mdn_handle* h, long long n_steps, int energy_mode);
-/* MD::make_pair for every replica now (used after re-centering). */
+/* MD::make_pair for every replica now, classifying against the ion centre
+ * of the current positions. */
 int  mdn_make_pair(mdn_handle* h);
 /* Re-centres every replica on its ion (src/run.cpp:42-53).  compat = 1 keeps
  * the reference's effect (only the ion centre entry is zeroed); compat = 0
- * shifts every position.  Then calls MD::make_pair.                        */
+ * shifts every position.  Then performs the MD::make_pair that MD::run calls
+ * next (src/run.cpp:54), against the centre entry as the shift left it, so
+ * no mdn_make_pair follows it.                                              */
 int  mdn_recenter(mdn_handle* h, int compat);
 /* Thermostat of one replica (replica < 0: all); MDN_NVT_OFF is MD::setNVE. */
 int  mdn_set_nvt(mdn_handle* h, int replica, int mode, double temperature);
@@ -324,6 +328,16 @@ int  mdn_kinetic(mdn_handle* h, double* out);
  * stream the kernels were launched on; kernel_launches = kernels issued.  */
 int  mdn_last_timing(mdn_handle* h, double* ms, long long* kernel_launches);
 int  mdn_set_launch(mdn_handle* h, int cluster_size, int threads, int steps_per_launch);
+/* The launch shape mdn_step uses: cluster size (the automatic choice when
+ * mdn_options.cluster_size is 0), threads per CTA, steps per launch. */
+int  mdn_get_launch(mdn_handle* h, int* cluster_size, int* threads, int* steps_per_launch);
+/* Launch-shape tuner: advances every replica by n_steps at each cluster size
+ * 1, 2, 4 and 8 (4 * n_steps steps in all), timing each block with CUDA
+ * events, and keeps the fastest size for later mdn_step calls; *best (may be
+ * NULL) receives it.  The steps are ordinary steps of the run: results do not
+ * depend on the launch shape.  A replica that fails during tuning is reported
+ * as mdn_step reports it.                                                   */
+int  mdn_tune_launch(mdn_handle* h, long long n_steps, int* best);
 /* Per-replica SM-cycle accounting of the step kernel: enable = 1 starts
  * accumulating (from zero), 0 stops.  out: [8*n_replicas] cycles per phase:
  * total, core integration, gas integration, rebuild, near gas molecules,

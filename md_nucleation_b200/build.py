@@ -1,4 +1,5 @@
-"""Builds the engine library in-tree: md_nucleation_b200/lib/libmdn.so.
+"""Builds in-tree: md_nucleation_b200/lib/libmdn.so (the engine),
+lib/libmdn_host.so and bin/mdn_run (the C++ host).
 
 nvcc compiles the CUDA sources for sm_100a only.  --fmad=false keeps FP64
 expressions rounding like the reference's x86 build; the FP32 pair kernels
@@ -15,6 +16,11 @@ CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libmdn.so")
 SOURCES = ["advance.cu", "snapshot.cu", "snapshot_noalloc.cu", "engine.cu"]
+HOST = os.path.join(HERE, "host")
+HOST_SOURCES = ["mdn_host.cpp"]
+HOST_LIB = os.path.join(LIB_DIR, "libmdn_host.so")
+BIN_DIR = os.path.join(HERE, "bin")
+HOST_BIN = os.path.join(BIN_DIR, "mdn_run")
 HEADERS = ["mdn_types.h", "device_util.cuh"]
 
 NVCC_FLAGS = [
@@ -40,16 +46,56 @@ def _stale():
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and not _stale():
-        return LIB
-    os.makedirs(LIB_DIR, exist_ok=True)
-    cmd = [nvcc()] + NVCC_FLAGS + ["-shared", "-I", os.path.join(ROOT, "include"), "-I", CSRC]
-    cmd += [os.path.join(CSRC, s) for s in SOURCES] + ["-o", LIB + ".tmp"]
+    if force or _stale():
+        os.makedirs(LIB_DIR, exist_ok=True)
+        cmd = [nvcc()] + NVCC_FLAGS + ["-shared", "-I", os.path.join(ROOT, "include"), "-I", CSRC]
+        cmd += [os.path.join(CSRC, s) for s in SOURCES] + ["-o", LIB + ".tmp"]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        os.replace(LIB + ".tmp", LIB)
+    build_host(force=force, verbose=verbose)
+    return LIB
+
+
+def cxx():
+    for c in ("/usr/bin/g++", os.environ.get("CXX"), shutil.which("g++")):
+        if c and os.path.exists(c):
+            return c
+    raise RuntimeError("g++ not found")
+
+
+def _host_stale():
+    outs = [HOST_LIB, HOST_BIN]
+    if not all(os.path.exists(o) for o in outs):
+        return True
+    t = min(os.path.getmtime(o) for o in outs)
+    deps = [os.path.join(HOST, f) for f in HOST_SOURCES + ["mdn_host.h", "mdn_run.cpp"]]
+    deps += [LIB, os.path.join(ROOT, "include", "mdn.h")]
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build_host(force: bool = False, verbose: bool = False):
+    """The C++ host: lib/libmdn_host.so (condition files, placement, run
+    cadence, output files) and bin/mdn_run (the command line), both linked
+    against lib/libmdn.so."""
+    if not force and not _host_stale():
+        return
+    os.makedirs(BIN_DIR, exist_ok=True)
+    inc = ["-I", os.path.join(ROOT, "include"), "-I", HOST]
+    lib = ["-L", LIB_DIR, "-lmdn", "-Wl,-rpath,$ORIGIN", "-Wl,-rpath,$ORIGIN/../lib"]
+    cmd = [cxx(), "-O2", "-std=c++17", "-fPIC", "-shared", "-Wall"] + inc
+    cmd += [os.path.join(HOST, f) for f in HOST_SOURCES] + ["-o", HOST_LIB + ".tmp"] + lib
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
-    os.replace(LIB + ".tmp", LIB)
-    return LIB
+    os.replace(HOST_LIB + ".tmp", HOST_LIB)
+    cmd = [cxx(), "-O2", "-std=c++17", "-Wall"] + inc + [os.path.join(HOST, "mdn_run.cpp"), "-o", HOST_BIN + ".tmp",
+                                                         "-L", LIB_DIR, "-lmdn_host"] + lib
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    os.replace(HOST_BIN + ".tmp", HOST_BIN)
 
 
 def ptxas_report() -> str:

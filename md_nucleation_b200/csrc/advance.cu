@@ -17,9 +17,9 @@
  *     a gas molecule interacts only with the core: molecules whose gas-ion /
  *     gas-vapor lists are empty ("far") are advanced by one thread in a single
  *     pass (kick, drift, intramolecular force, kick); "near" molecules are
- *     handled by one warp each, lanes striding over the list, with a
- *     warp-shuffle reduction of the molecule's force and fixed-point atomics
- *     for the reaction on the core.
+ *     handled by one thread each too, walking the molecule's lists (about one
+ *     entry per molecule), with shared-memory fixed-point atomics for the
+ *     reaction on the core.
  *
  * Each step follows MD::verlet (src/verlet.cpp:20-39) exactly:
  *   kick (MD::velocity_calculation), [MD::velocity_scaling], drift with
@@ -34,8 +34,8 @@
  * Precision: FP64 for integration, SHAKE, centres, weights, the rebuild and
  * the bonded terms; FP32 for the pair terms (LJ, Coulomb, Born-Mayer-Huggins)
  * on coordinates taken relative to the ion centre; every sum with more than one
- * writer is an int64 fixed-point sum (units 2^-32 kcal/mol/A for forces,
- * 2^-24 kcal/mol for energies), so results do not depend on the launch shape.
+ * writer is an int64 fixed-point sum (units 2^-40 kcal/mol/A for forces,
+ * 2^-36 kcal/mol for energies), so results do not depend on the launch shape.
  */
 #include <cooperative_groups.h>
 
@@ -614,6 +614,11 @@ __device__ __forceinline__ bool term_on(const Ctx& x, unsigned bit) {
   return (x.P->interactions & bit) && (!x.a->term_mask || (x.a->term_mask & bit));
 }
 
+/* Core pairs as tiles of 32 i atoms (one per lane) x 32 j atoms walked by
+ * the whole warp, so every j load is a shared-memory broadcast.  Every
+ * ordered pair (i, j) is evaluated on i's side (the full matrix): the i force
+ * stays in registers and reaches the core sums once per tile, with no
+ * reaction atomics; energies count each pair once (j > i). */
 __device__ void core_pairs(Ctx& x, bool eflag) {
   const RepParams* P = x.P;
   const int ni = P->n_ion, nc = x.n_core, nt = P->n_types;
@@ -622,93 +627,99 @@ __device__ void core_pairs(Ctx& x, bool eflag) {
   if (!(amber || bmh || vi || vv)) return;
   const float qqf = (float)P->qqrd2e;
   const int nblk = (nc + 31) >> 5;
-  const long long items = (long long)nc * nblk;
+  const int items = nblk * nblk;
+  const int lane = threadIdx.x & 31;
+  const int nwb = blockDim.x >> 5;
   const int* bmht = x.ib + P->o_ion_bmh;
-  long long eU[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  for (long long it = (long long)x.rank * blockDim.x + threadIdx.x; it < items;
-       it += (long long)x.C * blockDim.x) {
-    int i = (int)(it / nblk), jb = (int)(it - (long long)i * nblk);
-    float4 pi = x.c.pos[i];
-    int ti = x.c.type[i];
-    int mi = x.c.mol[i];
-    float wi = x.c.w[i];
-    bool iion = i < ni;
-    long long F[3] = {0, 0, 0};
-    int j1 = min(nc, (jb + 1) * 32);
-    for (int j = jb * 32; j < j1; j++) {
-      if (j == i) continue;
-      bool jion = j < ni;
-      float4 pj = x.c.pos[j];
-      float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-      float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      float fp = 0.0f, e = 0.0f;
-      int bucket = 0;
+  long long e_ion = 0, e_vi = 0, e_vv = 0;
+  for (int it = x.rank * nwb + (threadIdx.x >> 5); it < items; it += x.C * nwb) {
+    const int ib = it / nblk, jb = it - ib * nblk;
+    const int i = ib * 32 + lane;
+    const bool act = i < nc;
+    const int ii = act ? i : 0;
+    const float4 pi = x.c.pos[ii];
+    const int ti = x.c.type[ii], mi = x.c.mol[ii];
+    const float wi = x.c.w[ii];
+    const bool iion = ii < ni;
+    const int bi = (bmh && iion) ? bmht[ii] : 0;
+    long long F0 = 0, F1 = 0, F2 = 0;
+    const int j0 = jb * 32, j1 = min(nc, j0 + 32);
+    for (int j = j0; j < j1; j++) {
+      const float4 pj = x.c.pos[j];
+      const int tj = x.c.type[j], mj = x.c.mol[j];
+      const float wj = x.c.w[j];
+      if (!act || j == i) continue;
+      const bool jion = j < ni;
+      const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      float fp = 0.0f;
       bool any = false;
+      int bucket = 0;
       if (iion && jion) {
-        if (amber && !((x.c.excl[i * P->excl_words + (j >> 5)] >> (j & 31)) & 1u)) {
-          int tj = x.c.type[j];
+        const bool ex = amber && ((x.c.excl[i * P->excl_words + (j >> 5)] >> (j & 31)) & 1u);
+        if (amber && !ex) {
           float ee;
           fp += lj_coul(r2, x.c.ljA[ti * nt + tj], x.c.ljB[ti * nt + tj], qqf * pi.w * pj.w, true, &ee);
-          e += ee;
           any = true;
         }
         if (bmh) {
           float ee;
-          fp += born(r2, bmht[i], bmht[j], qqf * pi.w * pj.w, &ee);
-          e += ee;
+          fp += born(r2, bi, bmht[j], qqf * pi.w * pj.w, &ee);
           any = true;
         }
-        bucket = MDN_U_ION;
+        bucket = 1;
       } else if (iion != jion) {
         if (vi) {
-          int tj = x.c.type[j];
           float ee;
-          fp = lj_coul(r2, x.c.ljA[ti * nt + tj], x.c.ljB[ti * nt + tj], qqf * pi.w * pj.w, true, &ee) *
-               (wi * x.c.w[j]);
-          e = ee;
+          fp = lj_coul(r2, x.c.ljA[ti * nt + tj], x.c.ljB[ti * nt + tj], qqf * pi.w * pj.w, true, &ee) * (wi * wj);
           any = true;
-          bucket = MDN_U_VI;
+          bucket = 2;
         }
-      } else if (mi != x.c.mol[j]) {
+      } else if (mi != mj) {
         if (vv) {
-          int tj = x.c.type[j];
           float ee;
-          fp = lj_coul(r2, x.c.ljA[ti * nt + tj], x.c.ljB[ti * nt + tj], qqf * pi.w * pj.w, true, &ee) *
-               (wi * x.c.w[j]);
-          e = ee;
+          fp = lj_coul(r2, x.c.ljA[ti * nt + tj], x.c.ljB[ti * nt + tj], qqf * pi.w * pj.w, true, &ee) * (wi * wj);
           any = true;
-          bucket = MDN_U_VV;
+          bucket = 3;
         }
       }
       if (!any) continue;
-      F[0] += fixf(fp * dx);
-      F[1] += fixf(fp * dy);
-      F[2] += fixf(fp * dz);
+      F0 += fixf(fp * dx);
+      F1 += fixf(fp * dy);
+      F2 += fixf(fp * dz);
       if (eflag && j > i) {
         const double R2 = r2d(x.c.x + 3 * i, x.c.x + 3 * j);
         const double qi = i < ni ? x.db[P->d_ion_q + i] : x.db[P->d_vap_q + (i - ni) % P->a_v];
         const double qj = j < ni ? x.db[P->d_ion_q + j] : x.db[P->d_vap_q + (j - ni) % P->a_v];
         const double qq = P->qqrd2e * qi * qj;
-        const int tj = x.c.type[j];
         double ed = 0;
-        if (bucket == MDN_U_ION) {
+        if (bucket == 1) {
           if (amber && !((x.c.excl[i * P->excl_words + (j >> 5)] >> (j & 31)) & 1u))
             ed += lj_coul_energy(R2, x.db[P->d_ljA + ti * nt + tj], x.db[P->d_ljB + ti * nt + tj], qq);
-          if (bmh) ed += born_energy(R2, bmht[i], bmht[j], qq);
+          if (bmh) ed += born_energy(R2, bi, bmht[j], qq);
+          e_ion += efixd(ed);
         } else {
           ed = lj_coul_energy(R2, x.db[P->d_ljA + ti * nt + tj], x.db[P->d_ljB + ti * nt + tj], qq);
+          if (bucket == 2) e_vi += efixd(ed);
+          else e_vv += efixd(ed);
         }
-        eU[bucket] += efixd(ed);
       }
-      (void)e;
     }
-    if (F[0] | F[1] | F[2]) acc_add(x, i, F);
+    if (act && (F0 | F1 | F2)) {
+      const long long F[3] = {F0, F1, F2};
+      acc_add(x, i, F);
+    }
   }
-  if (eflag)
-    for (int b = 0; b < 8; b++) {
-      long long s = warp_sum_ll(eU[b]);
-      if ((threadIdx.x & 31) == 0) energy_add(x, b, s);
+  if (eflag) {
+    e_ion = warp_sum_ll(e_ion);
+    e_vi = warp_sum_ll(e_vi);
+    e_vv = warp_sum_ll(e_vv);
+    if (lane == 0) {
+      energy_add(x, MDN_U_ION, e_ion);
+      energy_add(x, MDN_U_VI, e_vi);
+      energy_add(x, MDN_U_VV, e_vv);
     }
+  }
 }
 
 __device__ void core_bonded(Ctx& x, bool eflag) {
@@ -782,35 +793,83 @@ __device__ __forceinline__ void partition(const Ctx& x, int n, int* lo, int* hi)
 }
 
 /* intramolecular bond force of one gas molecule (PotentialGasIntra), FP64 */
+/* Gas molecules have one or two atoms (AG); the bonded and SHAKE terms of a
+ * two-atom molecule copy the pair into fixed slots (swapped when a row reads
+ * (1, 0)) so that every array index is a compile-time constant and the
+ * arrays stay in registers.  The arithmetic is that of bond_fd / shake_pair
+ * on the row's own order. */
+template <int AG>
 __device__ __forceinline__ double gas_intra(const Ctx& x, const double* X, double* F) {
-  const RepParams* P = x.P;
-  double e = 0;
-  for (int b = 0; b < P->n_gas_bonds; b++) {
-    const int* row = x.ib + P->o_gas_bonds + 3 * b;
-    BondOut o;
-    bond_fd(X, x.db + P->d_bond + 2 * row[2], row[0], row[1], o);
-    for (int k = 0; k < 3; k++) {
-      F[3 * row[0] + k] += o.f[0][k];
-      F[3 * row[1] + k] += o.f[1][k];
+  if constexpr (AG == 1) {
+    return 0.0;
+  } else {
+    const RepParams* P = x.P;
+    double e = 0;
+    for (int b = 0; b < P->n_gas_bonds; b++) {
+      const int* row = x.ib + P->o_gas_bonds + 3 * b;
+      const bool sw = row[0] != 0;
+      double Y[6];
+      for (int k = 0; k < 3; k++) {
+        Y[k] = sw ? X[3 + k] : X[k];
+        Y[3 + k] = sw ? X[k] : X[3 + k];
+      }
+      BondOut o;
+      bond_fd(Y, x.db + P->d_bond + 2 * row[2], 0, 1, o);
+      for (int k = 0; k < 3; k++) {
+        F[k] += sw ? o.f[1][k] : o.f[0][k];
+        F[3 + k] += sw ? o.f[0][k] : o.f[1][k];
+      }
+      e += o.e;
     }
-    e += o.e;
+    return e;
   }
-  return e;
+}
+
+/* SHAKE of a two-atom gas molecule, the sweeps of shake_small with one colour */
+__device__ __forceinline__ int shake_gas2(const Ctx& x, double* X, const double* R, const double* m) {
+  const RepParams* P = x.P;
+  const int* rigid = x.ib + P->o_gas_rigid;
+  const int n = P->n_gas_rigid;
+  bool converge = false;
+  for (int sweep = 0; sweep < MDN_SHAKE_MAX_SWEEPS && !converge; sweep++) {
+    for (int k = 0; k < n; k++) {
+      const bool sw = rigid[3 * k] != 0;
+      double Y[6], RY[6];
+      for (int q = 0; q < 3; q++) {
+        Y[q] = sw ? X[3 + q] : X[q];
+        Y[3 + q] = sw ? X[q] : X[3 + q];
+        RY[q] = sw ? R[3 + q] : R[q];
+        RY[3 + q] = sw ? R[q] : R[3 + q];
+      }
+      shake_pair(Y, RY, 0, 1, x.db[P->d_bond + 2 * rigid[3 * k + 2] + 1], sw ? m[1] : m[0], sw ? m[0] : m[1]);
+      for (int q = 0; q < 3; q++) {
+        X[q] = sw ? Y[3 + q] : Y[q];
+        X[3 + q] = sw ? Y[q] : Y[3 + q];
+      }
+    }
+    converge = true;
+    for (int k = 0; k < n; k++)
+      if (shake_residual(X, 0, 1, x.db[P->d_bond + 2 * rigid[3 * k + 2] + 1]) > 1e-20) converge = false;
+  }
+  return converge ? 0 : MDN_ST_SHAKE_NOCONV;
 }
 
 /* kick + drift (+SHAKE) of the gas molecules of this CTA; far molecules also
  * get their intramolecular force and the second kick when `fused`. */
-__device__ void gas_integrate(Ctx& x, bool fused, bool eflag) {
+template <int AG>
+__device__ void gas_integrate_t(Ctx& x, bool fused, bool eflag) {
   const RepParams* P = x.P;
   const KArgs* a = x.a;
-  const int ag = P->a_g, par = x.D->parity;
+  constexpr int ag = AG;
+  const int par = x.D->parity;
   const bool sh = (P->interactions & MDN_I_SHAKE) && P->n_gas_rigid > 0;
   const bool vcorr = !(P->quirks & MDN_Q_SHAKE_NO_VCORR);
   const bool intra = term_on(x, MDN_I_GAS_INTRA) && P->n_gas_bonds > 0;
   const double dt = P->dt;
   int lo, hi;
   partition(x, x.D->n_gas_in, &lo, &hi);
-  double m[MDN_MAX_GAS_ATOMS], c2[MDN_MAX_GAS_ATOMS];
+  double m[AG], c2[AG];
+#pragma unroll
   for (int at = 0; at < ag; at++) {
     int t = x.ib[P->o_gas_type + at];
     m[at] = x.db[P->d_mass + t];
@@ -818,7 +877,7 @@ __device__ void gas_integrate(Ctx& x, bool fused, bool eflag) {
   }
   long long eg = 0;
   for (int s = lo + threadIdx.x; s < hi; s += blockDim.x) {
-    double X[3 * MDN_MAX_GAS_ATOMS], V[3 * MDN_MAX_GAS_ATOMS], F[3 * MDN_MAX_GAS_ATOMS], R[3 * MDN_MAX_GAS_ATOMS];
+    double X[3 * AG], V[3 * AG], F[3 * AG], R[3 * AG];
     for (int at = 0; at < ag; at++) {
       size_t g = gatom(P, par, s, at);
       for (int k = 0; k < 3; k++) {
@@ -834,20 +893,23 @@ __device__ void gas_integrate(Ctx& x, bool fused, bool eflag) {
         X[3 * at + k] = X[3 * at + k] + V[3 * at + k] * dt;
         F[3 * at + k] = 0.0;
       }
-    if (sh) {
-      double Xd[3 * MDN_MAX_GAS_ATOMS];
-      for (int q = 0; q < 3 * ag; q++) Xd[q] = X[q];
-      int zero = 0;
-      int st = shake_small(x, X, V, R, m, ag, x.ib + P->o_gas_rigid, P->n_gas_rigid, &zero, 1, false);
-      if (st) set_status(x, st);
-      if (vcorr)
-        for (int q = 0; q < 3 * ag; q++) V[q] += (X[q] - Xd[q]) / dt;
+    if constexpr (AG == 2) {
+      if (sh) {
+        double Xd[3 * AG];
+#pragma unroll
+        for (int q = 0; q < 3 * ag; q++) Xd[q] = X[q];
+        int st = shake_gas2(x, X, R, m);
+        if (st) set_status(x, st);
+        if (vcorr)
+#pragma unroll
+          for (int q = 0; q < 3 * ag; q++) V[q] += (X[q] - Xd[q]) / dt;
+      }
     }
     if (!isfinite(X[0] + X[1] + X[2] + V[0] + V[1] + V[2])) set_status(x, MDN_ST_NONFINITE);
     bool near = fused ? (a->near_gi[gmol(P, par, s)] >= 0) : true;
     if (!near) {
       if (intra) {
-        double e = gas_intra(x, X, F);
+        double e = gas_intra<AG>(x, X, F);
         if (eflag) eg += efixd(e);
       }
       for (int at = 0; at < ag; at++)
@@ -868,20 +930,28 @@ __device__ void gas_integrate(Ctx& x, bool fused, bool eflag) {
   }
 }
 
+__device__ void gas_integrate(Ctx& x, bool fused, bool eflag) {
+  if (x.P->a_g == 1) gas_integrate_t<1>(x, fused, eflag);
+  else gas_integrate_t<2>(x, fused, eflag);
+}
+
 /* after a rebuild: intramolecular force and second kick of the far molecules */
-__device__ void gas_far_pass(Ctx& x, bool eflag, bool kick) {
+template <int AG>
+__device__ void gas_far_pass_t(Ctx& x, bool eflag, bool kick) {
   const RepParams* P = x.P;
   const KArgs* a = x.a;
-  const int ag = P->a_g, par = x.D->parity;
+  constexpr int ag = AG;
+  const int par = x.D->parity;
   const bool intra = term_on(x, MDN_I_GAS_INTRA) && P->n_gas_bonds > 0;
   int lo, hi;
   partition(x, x.D->n_gas_in, &lo, &hi);
-  double c2[MDN_MAX_GAS_ATOMS];
+  double c2[AG];
+#pragma unroll
   for (int at = 0; at < ag; at++) c2[at] = x.c.c2[x.ib[P->o_gas_type + at]];
   long long eg = 0;
   for (int s = lo + threadIdx.x; s < hi; s += blockDim.x) {
     if (a->near_gi[gmol(P, par, s)] >= 0) continue;
-    double X[3 * MDN_MAX_GAS_ATOMS], F[3 * MDN_MAX_GAS_ATOMS];
+    double X[3 * AG], F[3 * AG];
     for (int at = 0; at < ag; at++) {
       size_t g = gatom(P, par, s, at);
       for (int k = 0; k < 3; k++) {
@@ -890,7 +960,7 @@ __device__ void gas_far_pass(Ctx& x, bool eflag, bool kick) {
       }
     }
     if (intra) {
-      double e = gas_intra(x, X, F);
+      double e = gas_intra<AG>(x, X, F);
       if (eflag) eg += efixd(e);
     }
     for (int at = 0; at < ag; at++) {
@@ -907,15 +977,22 @@ __device__ void gas_far_pass(Ctx& x, bool eflag, bool kick) {
   }
 }
 
+__device__ void gas_far_pass(Ctx& x, bool eflag, bool kick) {
+  if (x.P->a_g == 1) gas_far_pass_t<1>(x, eflag, kick);
+  else gas_far_pass_t<2>(x, eflag, kick);
+}
+
 /* near molecules (those with a gas-ion or gas-vapor list entry): one thread
  * each, walking the molecule's lists (about one entry per molecule in the
  * batched workload, so a wider split leaves lanes idle); the molecule's own
  * force stays in registers, the reaction goes to the core sums by shared
  * 64-bit integer atomics, so the result does not depend on the order */
-__device__ void gas_near_pass(Ctx& x, bool eflag, bool kick) {
+template <int AG>
+__device__ void gas_near_pass_t(Ctx& x, bool eflag, bool kick) {
   const RepParams* P = x.P;
   const KArgs* a = x.a;
-  const int ag = P->a_g, av = P->a_v, par = x.D->parity, nt = P->n_types, ni = P->n_ion;
+  constexpr int ag = AG;
+  const int av = P->a_v, par = x.D->parity, nt = P->n_types, ni = P->n_ion;
   const bool gi = term_on(x, MDN_I_GI), gv = term_on(x, MDN_I_GV);
   const bool intra = term_on(x, MDN_I_GAS_INTRA) && P->n_gas_bonds > 0;
   const int nj = (P->quirks & MDN_Q_GV_GAS_COUNT) ? min(ag, av) : av;
@@ -933,8 +1010,9 @@ __device__ void gas_near_pass(Ctx& x, bool eflag, bool kick) {
     while (L < H) { int M = (L + H) >> 1; if (nl[M] < hi) L = M + 1; else H = M; }
     b1 = L;
   }
-  int gtype[MDN_MAX_GAS_ATOMS];
-  double c2[MDN_MAX_GAS_ATOMS];
+  int gtype[AG];
+  double c2[AG];
+#pragma unroll
   for (int at = 0; at < ag; at++) {
     gtype[at] = x.ib[P->o_gas_type + at];
     c2[at] = x.c.c2[gtype[at]];
@@ -944,16 +1022,18 @@ __device__ void gas_near_pass(Ctx& x, bool eflag, bool kick) {
   for (int e = b0 + (int)threadIdx.x; e < b1; e += blockDim.x) {
     const int s = nl[e];
     const size_t ms = gmol(P, par, s);
-    float3 gp[MDN_MAX_GAS_ATOMS];
-    double X[3 * MDN_MAX_GAS_ATOMS];
+    float3 gp[AG];
+    double X[3 * AG];
+#pragma unroll
     for (int at = 0; at < ag; at++) {
       size_t g = gatom(P, par, s, at);
       for (int k = 0; k < 3; k++) X[3 * at + k] = a->slab_x[3 * g + k];
       gp[at] = make_float3((float)(X[3 * at] - com[0]), (float)(X[3 * at + 1] - com[1]),
                            (float)(X[3 * at + 2] - com[2]));
     }
-    long long F[MDN_MAX_GAS_ATOMS][3];
-    for (int at = 0; at < MDN_MAX_GAS_ATOMS; at++) F[at][0] = F[at][1] = F[at][2] = 0;
+    long long F[AG][3];
+#pragma unroll
+    for (int at = 0; at < AG; at++) F[at][0] = F[at][1] = F[at][2] = 0;
     if (gi) {
       const int start = a->near_gi[ms], cnt = a->gil_n[ms];
       for (int q = 0; q < cnt; q++) {
@@ -1001,14 +1081,15 @@ __device__ void gas_near_pass(Ctx& x, bool eflag, bool kick) {
         }
       }
     }
-    double Fd[3 * MDN_MAX_GAS_ATOMS];
+    double Fd[3 * AG];
+#pragma unroll
     for (int at = 0; at < ag; at++)
       for (int k = 0; k < 3; k++) {
         Fd[3 * at + k] = (double)F[at][k] * MDN_FIX_INV;
         if (!(fabs(Fd[3 * at + k]) < MDN_FIX_LIMIT)) set_status(x, MDN_ST_FIXED_OVERFLOW);
       }
     if (intra) {
-      double ei = gas_intra(x, X, Fd);
+      double ei = gas_intra<AG>(x, X, Fd);
       if (eflag) eintra += efixd(ei);
     }
     for (int at = 0; at < ag; at++) {
@@ -1029,6 +1110,11 @@ __device__ void gas_near_pass(Ctx& x, bool eflag, bool kick) {
       energy_add(x, MDN_U_GAS, eintra);
     }
   }
+}
+
+__device__ void gas_near_pass(Ctx& x, bool eflag, bool kick) {
+  if (x.P->a_g == 1) gas_near_pass_t<1>(x, eflag, kick);
+  else gas_near_pass_t<2>(x, eflag, kick);
 }
 
 /* sum of the core partials over the cluster -> f (double), identical in every CTA */

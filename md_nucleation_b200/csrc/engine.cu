@@ -126,6 +126,7 @@ struct mdn_handle {
   int* n_events = nullptr;
   int ev_cap = 65536;
   int* status = nullptr;
+  int auto_cluster = 1;  /* cluster size when mdn_options.cluster_size is 0 */
   int* job_order = nullptr;
   int* job_counter = nullptr;
   std::vector<int> order;
@@ -244,7 +245,7 @@ long long launch(mdn_handle* h, int mode, long long n_steps, int energy_mode, un
   a.nc_cap = h->nc_cap;
   a.nt_cap = h->nt_cap;
   a.excl_cap = h->excl_cap;
-  const int C = std::max(1, std::min(8, h->opt.cluster_size > 0 ? h->opt.cluster_size : 1));
+  const int C = std::max(1, std::min(8, h->opt.cluster_size > 0 ? h->opt.cluster_size : h->auto_cluster));
   int clusters = std::max(1, h->num_sms / C);
   clusters = std::min(clusters, (int)J.size());
   cudaLaunchConfig_t cfg;
@@ -306,7 +307,7 @@ void mdn_default_options(mdn_options* o) {
   memset(o, 0, sizeof *o);
   o->quirks = MDN_Q_ALL;
   o->force_mode = 0;
-  o->cluster_size = 1;
+  o->cluster_size = 0;
   o->threads = 512;
   o->steps_per_launch = 0;
   o->use_graph = 0;
@@ -334,7 +335,7 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
   if (opt.threads <= 0) opt.threads = 512;
   if (opt.threads % 32 || opt.threads > 512) return fail(MDN_ERR_ARG, "threads must be a multiple of 32 <= 512");
   if (opt.capacity_factor < 1.0) opt.capacity_factor = 1.0;
-  if (opt.cluster_size <= 0) opt.cluster_size = 1;
+  if (opt.cluster_size < 0 || opt.cluster_size > 8) return fail(MDN_ERR_ARG, "cluster size must be 0..8");
   if (opt.device < 0 || opt.device >= ndev) return fail(MDN_ERR_ARG, "bad device ordinal");
 
   mdn_handle* h = new mdn_handle();
@@ -602,6 +603,20 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
   h->order.resize(R);
   for (int r = 0; r < R; r++) h->order[r] = r;
   std::stable_sort(h->order.begin(), h->order.end(), [&](int a, int b) { return h->P[a].work > h->P[b].work; });
+  /* automatic cluster size: the smallest power of two that lets the largest
+   * replica finish within the time of an even share of the SMs
+   * (num_sms * W_max / W_total CTAs), at most 8 */
+  {
+    double wmax = 0, wsum = 0;
+    for (int r = 0; r < R; r++) {
+      wmax = std::max(wmax, h->P[r].work);
+      wsum += h->P[r].work;
+    }
+    const double want = wsum > 0 ? h->num_sms * wmax / wsum : 1.0;
+    int c = 1;
+    while (c < 8 && c < want) c *= 2;
+    h->auto_cluster = c;
+  }
 
 #define ALLOC(ptr, count)                                                          \
   do {                                                                             \
@@ -1278,6 +1293,33 @@ int mdn_profile(mdn_handle* h, int enable, long long* out) {
   if (enable && !h->prof_on) CK(cudaMemset(h->d_prof, 0, sizeof(long long) * MDN_PROF_N * h->R));
   h->prof_on = enable != 0;
   return MDN_OK;
+}
+
+int mdn_get_launch(mdn_handle* h, int* cluster_size, int* threads, int* steps_per_launch) {
+  if (!h) return fail(MDN_ERR_ARG, "null handle");
+  if (cluster_size) *cluster_size = h->opt.cluster_size > 0 ? h->opt.cluster_size : h->auto_cluster;
+  if (threads) *threads = h->opt.threads;
+  if (steps_per_launch) *steps_per_launch = h->opt.steps_per_launch;
+  return MDN_OK;
+}
+
+int mdn_tune_launch(mdn_handle* h, long long n_steps, int* best) {
+  if (!h || n_steps <= 0) return fail(MDN_ERR_ARG, "bad arguments");
+  int best_c = 0, status = MDN_OK;
+  float best_ms = 0;
+  for (int c = 1; c <= 8; c *= 2) {
+    h->opt.cluster_size = c;
+    int rc = mdn_step(h, n_steps, 0);
+    if (rc == MDN_ERR_REPLICA) status = rc;
+    else if (rc != MDN_OK) return rc;
+    if (best_c == 0 || h->last_ms < best_ms) {
+      best_c = c;
+      best_ms = h->last_ms;
+    }
+  }
+  h->opt.cluster_size = best_c;
+  if (best) *best = best_c;
+  return status;
 }
 
 int mdn_set_launch(mdn_handle* h, int cluster_size, int threads, int steps_per_launch) {

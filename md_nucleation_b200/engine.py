@@ -61,6 +61,8 @@ def lib():
         L.mdn_kinetic.argtypes = [vp, C.POINTER(C.c_double)]
         L.mdn_last_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
         L.mdn_set_launch.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+        L.mdn_get_launch.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.mdn_tune_launch.argtypes = [vp, C.c_longlong, C.POINTER(C.c_int)]
         L.mdn_snapshot.argtypes = [vp, C.POINTER(C.c_longlong), C.c_longlong, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.POINTER(C.c_double)]
         L.mdn_host_alloc.argtypes = [C.c_size_t, C.POINTER(C.c_void_p)]
@@ -195,6 +197,19 @@ class Engine:
 
     def compute_forces(self, term_mask: int = 0):
         _ck(self.L.mdn_compute_forces(self.h, term_mask))
+
+    def get_launch(self):
+        """(cluster size, threads per CTA, steps per launch) of mdn_step."""
+        c, t, n = C.c_int(), C.c_int(), C.c_int()
+        _ck(self.L.mdn_get_launch(self.h, C.byref(c), C.byref(t), C.byref(n)))
+        return c.value, t.value, n.value
+
+    def tune_launch(self, n_steps: int = 100) -> int:
+        """Runs n_steps at each cluster size 1, 2, 4, 8 and keeps the fastest
+        (mdn_tune_launch); returns it.  The steps advance the replicas."""
+        best = C.c_int(0)
+        _ck(self.L.mdn_tune_launch(self.h, n_steps, C.byref(best)))
+        return best.value
 
     def set_launch(self, cluster_size=0, threads=0, steps_per_launch=-1):
         _ck(self.L.mdn_set_launch(self.h, cluster_size, threads, steps_per_launch))

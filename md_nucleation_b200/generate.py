@@ -19,6 +19,7 @@ radians; dihedral types hold three (K, n, d) terms as in readIonFile
 from __future__ import annotations
 
 import math
+import os
 from dataclasses import dataclass
 from typing import List, Optional
 
@@ -370,10 +371,11 @@ def assemble(ion: Species, gas: Species, vap: Species, *, gas_name: str, n_gas: 
 
     The gas molecule's COM mass is the sum of its atoms' masses, so that the
     centre-of-mass bookkeeping and the atom masses agree.  reference_masses=True
-    takes the reference's hard-coded molecular mass instead
-    (src/pairList/updateGasIn.cpp, src/initialization/initializationGas.cpp:
-    He 4.027 vs the atom's 4.0026, Ar 28.02 vs 39.948), which puts an argon
-    molecule's COM velocity 30% off its atom's."""
+    takes the reference's molecular mass instead (src/constants.hpp:34,
+    used by src/initialization/initializationGas.cpp:61): 4.0026 for He, whose
+    atom is 4.027, and 39.948 for Ar, whose atom is 28.02
+    (src/initialization/setCondition.cpp:50,104); the argon centre of mass
+    then moves 30% off its atom."""
     offs_t, offs_b, offs_a, offs_d = [0], [0], [0], [0]
     mass, eps, sig, names = [], [], [], []
     bc, ac, dm, dc = [], [], [], []
@@ -544,3 +546,109 @@ def small_system(seed: int = 7, gas: str = "N2", vapor: str = "methanol", ion: s
                     n_gas=n_gas, n_vap=n_vap, T=300.0, p=p, dt=dt, interactions=interactions,
                     seed=seed, shake_h=shake_h, rng=rng, nvt_mode=nvt_mode,
                     min_dist=min(10.0, 0.5 * n_dens ** (-1 / 3)), box=box, label="small")
+
+
+# --------------------------------------------------------------------------
+# input files in the reference's own format
+# --------------------------------------------------------------------------
+# type codes the reference's readers turn back into element names
+# (src/initialization/readIonFile.cpp:49-67): C, N, O, H; Na stays "Na",
+# "cl" becomes "Cl"
+_CODE_BY_MASS = {12.011: "#c3", 14.007: "#n3", 15.999: "#os", 1.008: "#hc", 22.99: "Na", 35.45: "cl"}
+_CODE_BY_NAME = {"Na": "Na", "Cl": "cl", "OW": "#ow", "O": "#oh", "HO": "#ho", "HW": "#hw", "HC": "#hc",
+                 "H": "#hc", "C": "#c3", "N": "#n3"}
+
+
+def _type_code(sp: Species, t: int) -> str:
+    name = sp.names[t]
+    if name in _CODE_BY_NAME:
+        return _CODE_BY_NAME[name]
+    if t in sp.h_types:
+        return "#hc"
+    return _CODE_BY_MASS.get(round(float(sp.mass[t]), 3), name)
+
+
+def write_molecule_file(path: str, sp: Species) -> None:
+    """One ion or vapor file as Variables::readIonFile / readVaporFile read
+    it (src/initialization/readIonFile.cpp:30-156): tab-separated sections,
+    1-based indices.  Angles are written in degrees."""
+    f = repr
+    out = ["atom type"]
+    for t in range(len(sp.names)):
+        out.append(f"{t + 1}\t{_type_code(sp, t)}\t{f(float(sp.mass[t]))}\t{f(float(sp.eps[t]))}\t"
+                   f"{f(float(sp.sigma[t]))}")
+    if len(sp.bond_coeff):
+        out += ["", "bond type"]
+        for b, (K, r0) in enumerate(np.asarray(sp.bond_coeff, float)):
+            out.append(f"{b + 1}\tb{b + 1}\t{f(float(K))}\t{f(float(r0))}")
+    if len(sp.angle_coeff):
+        out += ["", "angle type"]
+        for a, (K, th) in enumerate(np.asarray(sp.angle_coeff, float)):
+            out.append(f"{a + 1}\ta{a + 1}\t{f(float(K))}\t{f(float(th) * 180.0 / math.pi)}")
+    if len(sp.dih_multi):
+        out += ["", "dihedral type"]
+        for d, (m, row) in enumerate(zip(np.asarray(sp.dih_multi), np.asarray(sp.dih_coeff, float))):
+            terms = "\t".join(f"{f(float(row[5 * k]))}\t{f(float(row[5 * k + 1]))}\t{f(float(row[5 * k + 2]))}"
+                              for k in range(3))
+            out.append(f"{d + 1}\td{d + 1}\t{int(m)}\t{terms}")
+    top = sp.top
+    out += ["", "atoms"]
+    x = np.asarray(top.x, float).reshape(-1, 3)
+    for i in range(top.n):
+        out.append(f"{i + 1}\t{int(top.type[i]) + 1}\t{f(float(top.charge[i]))}\t"
+                   f"{f(float(x[i, 0]))}\t{f(float(x[i, 1]))}\t{f(float(x[i, 2]))}")
+    bonds = [list(b) for b in np.asarray(top.bonds, int).reshape(-1, 3)]
+    bonds += [list(b) for b in np.asarray(top.rigid, int).reshape(-1, 3)]
+    if bonds:
+        out += ["", "bonds"]
+        out += [f"{i + 1}\t{j + 1}\t{t + 1}" for i, j, t in bonds]
+    ang = np.asarray(top.angles, int).reshape(-1, 4)
+    if len(ang):
+        out += ["", "angles"]
+        out += [f"{i + 1}\t{j + 1}\t{k + 1}\t{t + 1}" for i, j, k, t in ang]
+    dih = np.asarray(top.dihedrals, int).reshape(-1, 5)
+    if len(dih):
+        out += ["", "dihedrals"]
+        out += [f"{i + 1}\t{j + 1}\t{k + 1}\t{l + 1}\t{t + 1}" for i, j, k, l, t in dih]
+    with open(path, "w") as fh:
+        fh.write("\n".join(out) + "\n")
+
+
+def write_reference_inputs(directory: str, ion: Species, vapor: Species, *, gas: str, n_gas: int, n_vapor: int,
+                           T: float = 300.0, p: float = 1e5, dt: float = 1.0, total_steps: int = 1000,
+                           relax_steps: int = 0, observe: int = 100, interactions: int = 0,
+                           shake_h: bool = False, nvt: str = "OFF", output: str = "dump",
+                           efield=None) -> str:
+    """Writes ion.txt, vapor.txt and cond.txt under `directory` in the
+    reference's formats (MD::readCondFile, src/initialization/setCondition.cpp:4-254)
+    and returns the condition file's path.  `interactions` takes MDN_I_* bits
+    (gi, gv, vi, vv, gg, AMBER or BMH for the ion); nvt is "OFF", "scale" or a
+    temperature."""
+    os.makedirs(directory, exist_ok=True)
+    ion_path = os.path.join(directory, "ion.txt")
+    vap_path = os.path.join(directory, "vapor.txt")
+    write_molecule_file(ion_path, ion)
+    write_molecule_file(vap_path, vapor)
+    I = interactions
+    lines = [f"Input {ion_path}", f"Vapor {vap_path} {n_vapor}", f"Gas {gas} {n_gas}",
+             f"Temperature {T!r}", f"Pressure {p!r}", f"dt {dt!r}", f"TotalSteps {total_steps}",
+             f"RelaxSteps {relax_steps}", f"Output {os.path.join(directory, output)} {observe}",
+             f"NVTion {nvt}"]
+    if shake_h:
+        lines.append("SHAKE H")
+    lines.append("Interactions")
+    if I & abi.I_AMBER:
+        lines.append(" ion AMBER")
+    if I & abi.I_BMH:
+        lines.append(" ion Born-Mayer-Huggins-NaCl")
+    lines.append(f" gg {'LJ' if I & abi.I_GG else 'OFF'}")
+    lines.append(f" gi {'LJ' if I & abi.I_GI else 'OFF'}")
+    lines.append(f" vi {'LJcoul' if I & abi.I_VI else 'OFF'}")
+    lines.append(f" vv {'LJcoul' if I & abi.I_VV else 'OFF'}")
+    lines.append(f" gv {'LJ' if I & abi.I_GV else 'OFF'}")
+    if efield is not None:
+        lines.append(" Efield " + " ".join(repr(float(e)) for e in efield))
+    cond = os.path.join(directory, "cond.txt")
+    with open(cond, "w") as fh:
+        fh.write("\n".join(lines) + "\n")
+    return cond

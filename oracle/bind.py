@@ -203,6 +203,22 @@ class OracleReplica:
         if not self.h:
             raise RuntimeError("orc_create failed")
 
+    @classmethod
+    def from_desc(cls, desc_ptr, quirks: int = abi.Q_ALL, force_mode: int = 0):
+        """A replica from a descriptor built elsewhere (the C++ host's
+        mdnh_desc); desc_ptr must outlive the replica."""
+        from types import SimpleNamespace as NS
+        d = desc_ptr.contents
+        o = cls.__new__(cls)
+        o.spec = NS(ion=NS(n=d.ion.n_atoms), gas=NS(n=d.gas.n_atoms), vapor=NS(n=d.vapor.n_atoms),
+                    n_gas=d.n_gas, n_vapor=d.n_vapor)
+        o.L = orc_lib()
+        o._desc, o._keep = desc_ptr, None
+        o.h = o.L.orc_create(desc_ptr, quirks, force_mode)
+        if not o.h:
+            raise RuntimeError("orc_create failed")
+        return o
+
     def close(self):
         if self.h:
             self.L.orc_destroy(self.h)

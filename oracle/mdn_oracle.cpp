@@ -38,6 +38,8 @@
  *       gives vz (the second normal is unused)
  *     purpose 1, word 0: insertion angles a, b, c = 2 pi u01(w0..w2)
  *     purpose 1, word 1: N2 spin normals (vy_rot, vz_rot) from (w0, w1)
+ *     purpose 1, word 1 + t (t = 1..3): insertion angles of the t-th re-draw
+ *       of the checked insertion (MDN_Q_BLIND_INSERT cleared)
  *
  * SHAKE: the reference's iteration (src/shake.cpp:44-92) scales each
  * correction by (1/mi + 1/mj)^2 relative to the textbook multiplier

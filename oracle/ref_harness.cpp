@@ -606,7 +606,157 @@ void ref_export_dump(void* hp, const char* path, double time_fs) {
 
 }  // extern "C"
 
+namespace {
+
+/* minimal JSON writer for ref_read_inputs */
+struct Json {
+  std::string s;
+  void num(double v) {
+    char b[64];
+    snprintf(b, sizeof b, "%.17g", v);
+    s += b;
+  }
+  void str(const std::string& v) {
+    s += '"';
+    for (char c : v) {
+      if (c == '"' || c == '\\') s += '\\';
+      s += c;
+    }
+    s += '"';
+  }
+  void key(const char* k) {
+    if (!s.empty() && s.back() != '{' && s.back() != '[') s += ',';
+    str(k);
+    s += ':';
+  }
+  template <class V>
+  void arr(const V& v) {
+    s += '[';
+    bool first = true;
+    for (const auto& e : v) {
+      if (!first) s += ',';
+      first = false;
+      num((double)e);
+    }
+    s += ']';
+  }
+  template <class V>
+  void rows(const V& v) {
+    s += '[';
+    bool first = true;
+    for (const auto& r : v) {
+      if (!first) s += ',';
+      first = false;
+      arr(r);
+    }
+    s += ']';
+  }
+};
+
+}  // namespace
+
 extern "C" {
+/* Runs the reference's own readers on a condition file and the files it
+ * names -- MD::readCondFile (src/initialization/setCondition.cpp:4-254),
+ * Variables::readIonFile (src/initialization/readIonFile.cpp:3-179) and
+ * Variables::readVaporFile (src/initialization/readVaporFile.cpp:3-131), in
+ * MD::MD's order -- and writes what they stored as JSON into buf.  Returns
+ * the length, or -1 when buf is too small. */
+int ref_read_inputs(const char* cond, int calc, char* buf, int cap) {
+  MD* md = new MD(nullptr, calc);
+  md->readCondFile((char*)cond);
+  Variables* v = md->vars;
+  v->readIonFile(md->atomFile);
+  v->readVaporFile(md->vaporFile);
+  FLAG* f = md->flags;
+  Json j;
+  j.s = "{";
+  j.key("T"); j.num(md->T);
+  j.key("p"); j.num(md->p);
+  j.key("dt"); j.num(md->dt);
+  j.key("cutoff"); j.num(md->CUTOFF);
+  j.key("margin"); j.num(md->MARGIN);
+  j.key("box"); j.num(md->d_size);
+  j.key("total"); j.num((double)md->Noftimestep);
+  j.key("relax"); j.num((double)md->step_relax);
+  j.key("observe"); j.num(md->OBSERVE);
+  j.key("gastype"); j.num(md->gastype);
+  j.key("n_gas"); j.num(md->Nof_around_gas);
+  j.key("n_vapor"); j.num(md->Nof_around_vapor);
+  j.key("dump_path"); j.str(md->pp->dump_path ? md->pp->dump_path : "");
+  j.key("Tnh_ion"); j.num(md->pp->Tnh_ion);
+  j.key("Ecoeff"); j.arr(std::vector<double>{md->Ecoeff[0], md->Ecoeff[1], md->Ecoeff[2]});
+  j.key("flags"); j.s += "{";
+  j.key("force_lj"); j.num(f->force_lj);
+  j.key("inter_vi"); j.num(f->inter_vi);
+  j.key("inter_vv"); j.num(f->inter_vv);
+  j.key("inter_vg"); j.num(f->inter_vg);
+  j.key("inter_gg"); j.num(f->inter_gg);
+  j.key("intra_AMBER"); j.num(f->intra_AMBER);
+  j.key("force_born"); j.num(f->force_born);
+  j.key("efield"); j.num(f->efield);
+  j.key("gas_intra"); j.num(f->gas_intra);
+  j.key("vapor_intra"); j.num(f->vapor_intra);
+  j.key("shakeH"); j.num(f->shakeH ? 1 : 0);
+  j.key("nose_hoover_ion"); j.num(f->nose_hoover_ion);
+  j.key("velocity_scaling"); j.num(f->velocity_scaling);
+  j.s += "}";
+  j.key("atypes"); j.s += "[";
+  for (size_t t = 0; t < v->atypes.size(); t++) {
+    if (t) j.s += ",";
+    j.s += "[";
+    j.str(v->atypes[t].name);
+    j.s += ",";
+    j.num(v->atypes[t].mass);
+    j.s += ",";
+    j.num(v->atypes[t].coeff1);
+    j.s += ",";
+    j.num(v->atypes[t].coeff2);
+    j.s += "]";
+  }
+  j.s += "]";
+  std::vector<std::vector<double>> bt, ct, dt;
+  for (auto& b : v->btypes) bt.push_back({b.coeff[0], b.coeff[1]});
+  for (auto& c : v->ctypes) ct.push_back({c.coeff[0], c.coeff[1]});
+  for (auto& d : v->dtypes) {
+    std::vector<double> r{(double)d.multi};
+    for (int k = 0; k < 15; k++) r.push_back(d.coeff[k]);
+    dt.push_back(r);
+  }
+  j.key("btypes"); j.rows(bt);
+  j.key("ctypes"); j.rows(ct);
+  j.key("dtypes"); j.rows(dt);
+  j.key("ion"); j.s += "{";
+  j.key("type"); j.arr(v->typeAtom[0]);
+  j.key("charge"); j.arr(v->chargeAtom[0]);
+  j.key("x"); j.rows(v->positionAtom[0]);
+  j.key("bonds"); j.rows(v->bonds[0]);
+  j.key("rigid"); j.rows(v->rigid_pairs[0]);
+  j.key("angles"); j.rows(v->angles[0]);
+  j.key("dihedrals"); j.rows(v->dihedrals[0]);
+  j.s += "}";
+  j.key("vapor"); j.s += "{";
+  j.key("type"); j.arr(v->typeVapor);
+  j.key("charge"); j.arr(v->chargeVapor);
+  j.key("x"); j.rows(v->positionVapor);
+  j.key("bonds"); j.rows(v->bondsVapor);
+  j.key("rigid"); j.rows(v->bondsVaporRigid);
+  j.key("angles"); j.rows(v->anglesVapor);
+  j.key("dihedrals"); j.rows(v->dihedralsVapor);
+  j.s += "}";
+  j.key("gas"); j.s += "{";
+  j.key("type"); j.arr(v->typeGas);
+  j.key("charge"); j.arr(v->chargeGas);
+  j.key("x"); j.rows(v->positionGas);
+  j.key("bonds"); j.rows(v->bondsGas);
+  j.s += "}";
+  j.s += "}";
+  delete md;
+  if ((int)j.s.size() + 1 > cap) return -1;
+  memcpy(buf, j.s.c_str(), j.s.size() + 1);
+  return (int)j.s.size();
+}
+
 /* The reference's replica model (src/main.cpp:22-29): one replica per OpenMP
  * thread, each running MD::verlet n times.  threads <= 0: all threads.
  * MD::verlet never calls the reference's SHAKE (src/verlet.cpp:24); its
