@@ -72,6 +72,51 @@ def in_domain_atoms(infos, specs):
                     np.int64)
 
 
+# Algorithmic HBM bytes (the byte model of a streaming implementation):
+# per in-domain atom-step 164 B of integration (read x, v FP64, fixed-point F,
+# 1/m; write x, v, the float4 copy, a zeroed F) + 40 B of forces (float4 read,
+# F write), 4 B per pair-list entry and step, and per rebuild 72 B per
+# molecule (centre read, free flight and resampling write).
+BYTES_PER_ATOM_STEP = 164 + 40
+BYTES_PER_LIST_ENTRY = 4
+BYTES_PER_MOLECULE_REBUILD = 72
+
+
+def algorithmic_bytes(infos0, infos1, specs, md_steps):
+    """Bytes of the byte model over md_steps steps of every replica."""
+    b = 0.0
+    for i0, i1, s in zip(infos0, infos1, specs):
+        atoms = 0.5 * ((i0.n_ion + i0.n_gas_in * s.gas.n + i0.n_vapor_in * s.vapor.n) +
+                       (i1.n_ion + i1.n_gas_in * s.gas.n + i1.n_vapor_in * s.vapor.n))
+        lists = 0.5 * ((i0.gi_pairs + i0.gv_pairs) + (i1.gi_pairs + i1.gv_pairs))
+        b += md_steps * (atoms * BYTES_PER_ATOM_STEP + lists * BYTES_PER_LIST_ENTRY)
+        b += (i1.n_rebuilds - i0.n_rebuilds) * (1 + s.n_gas + s.n_vapor) * BYTES_PER_MOLECULE_REBUILD
+    return b
+
+
+def traffic_per_atom_step():
+    """DRAM bytes (read + write) per in-domain atom-step of mdn_advance: the
+    `dram_bytes_per_atom_step:` line of the ncu summary in
+    profiles/mdn_advance_batched.md, or None."""
+    import re
+    try:
+        with open(os.path.join(HERE, "profiles", "mdn_advance_batched.md")) as f:
+            m = re.search(r"dram_bytes_per_atom_step:\s*([0-9.eE+-]+)", f.read())
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+def measured_hbm_peak():
+    """(GB/s, source): the copy bandwidth measured on these GPUs, else the
+    earlier measurement on the same pool."""
+    try:
+        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured copy bandwidth (MEASURED_PEAKS.json)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback 6.65 TB/s"
+
+
 def algorithmic_flops(infos, specs):
     """FP32 flops of one MD step's pair terms, each pair once:
     gas-ion (gas atom x ion atom of listed molecule pairs, LJ), gas-vapor
@@ -343,8 +388,13 @@ def run_engine(args):
 
     # warm-up: the launch-shape tuner (4 blocks of MD_STEPS, one per cluster
     # size; results do not depend on the shape), then the warm-up steps
-    tuned = eng.tune_launch(MD_STEPS)
-    log(f"rank {rank}: tuned cluster size {tuned}")
+    if args.cluster:
+        eng.set_launch(args.cluster)
+        chosen_by = "--cluster"
+    else:
+        tuned = eng.tune_launch(MD_STEPS)
+        chosen_by = "mdn_tune_launch during warm-up"
+        log(f"rank {rank}: tuned cluster size {tuned}")
     for _ in range(args.warmup):
         eng.step(MD_STEPS)
     barrier()
@@ -374,6 +424,8 @@ def run_engine(args):
     value = atom_steps_all / (ms_max * 1e-3)
     flops_per_md_step = 0.5 * (flops0 + flops1)
     achieved_tflops = flops_per_md_step * MD_STEPS * args.steps / (ms_total * 1e-3) / 1e12
+    bytes_timed = algorithmic_bytes(infos0, infos1, specs, MD_STEPS * args.steps)
+    achieved_gbs = bytes_timed / (ms_total * 1e-3) / 1e9
     clocks = clk.summary()
 
     # end to end through the C ABI: per bench step the thermostat controls go
@@ -421,29 +473,39 @@ def run_engine(args):
                 "parallelism": f"replicas sharded over {ws} GPU(s), no collective in the step",
                 "launch": {"cluster_ctas_per_replica": launch_shape[0], "threads_per_cta": launch_shape[1],
                            "md_steps_per_launch": MD_STEPS if launch_shape[2] <= 0 else launch_shape[2],
-                           "chosen_by": "mdn_tune_launch during warm-up"},
+                           "chosen_by": chosen_by},
             },
             "roofline": {
-                "bound": "fp32", "achieved": achieved_tflops,
-                "peak": None, "unit": "TFLOP/s", "frac": None, "traffic": None,
-                "kernel": "mdn_advance",
-                "algorithmic_flops_per_md_step": flops_per_md_step,
+                "bound": "hbm", "achieved": achieved_gbs, "peak": None, "unit": "GB/s", "frac": None,
+                "traffic": None, "kernel": "mdn_advance",
+                "algorithmic_bytes_per_launch": bytes_timed / args.steps,
+                "launch": f"{MD_STEPS} MD steps of every replica",
+                "fp32": {"achieved": achieved_tflops, "unit": "TFLOP/s",
+                         "algorithmic_flops_per_md_step": flops_per_md_step},
             },
             "gpu_launches": launches,
             "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d_per_step,
                     "d2h_bytes_per_step": int(d2h / e2e_steps)},
         }
+        hbm, hbm_src = measured_hbm_peak()
+        out["roofline"]["peak"] = hbm
+        out["roofline"]["frac"] = achieved_gbs / hbm
+        out["roofline"]["peak_source"] = hbm_src
+        # DRAM bytes of one launch from ncu (a 32-replica capture scaled by
+        # atom-steps; profiles/mdn_advance_batched.md)
+        traffic = traffic_per_atom_step()
+        if traffic is not None:
+            out["roofline"]["traffic"] = traffic * atom_steps / args.steps
         # FP32 peak: 148 SMs x 128 FP32 lanes x 2 flops (FMA) at the SM clock
         # measured during the timed region (no FP32 figure is measured
         # separately on these GPUs)
         props = torch.cuda.get_device_properties(device)
         mhz = clocks["sm_mhz"] or 1965.0
         peak = props.multi_processor_count * 128 * 2 * mhz * 1e6 / 1e12
-        out["roofline"]["peak"] = peak
-        out["roofline"]["frac"] = achieved_tflops / peak
-        out["roofline"]["peak_source"] = (f"{props.multi_processor_count} SMs x 128 FP32 lanes x 2 "
-                                          f"at the measured {mhz:.0f} MHz")
+        out["roofline"]["fp32"].update({"peak": peak, "frac": achieved_tflops / peak,
+                                        "peak_source": f"{props.multi_processor_count} SMs x 128 lanes x 2 "
+                                                       f"at the measured {mhz:.0f} MHz"})
     # the plain one-system-per-launch path on the same GPU (rank 0, N = 1)
     if rank == 0 and ws == 1 and not args.no_plain:
         pv, psample = plain_sample(engine, specs, checked, args.plain_replicas)
@@ -478,6 +540,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the one-system-per-launch measurement")
     ap.add_argument("--plain-replicas", type=int, default=16)
+    ap.add_argument("--cluster", type=int, default=0, help="CTAs per replica (1..8); 0 = tuned in the warm-up")
     args = ap.parse_args()
     if args.warmup < 3 and not os.environ.get("MDN_BENCH_ALLOW_SHORT"):
         raise SystemExit("bench.py: --warmup must be >= 3")
