@@ -314,6 +314,30 @@ def plain_sample(engine, specs, quirks, n_pick: int):
     return atom_steps / seconds, sample
 
 
+def adjoint_measurement(engine):
+    """The gradient harness on the adjoint configuration: a 2,000-step window
+    of the production system (150-atom +1 chain, 100 methanol, 100,000 rigid
+    N2, SHAKE on X-H bonds, 300 K, 1e5 Pa) with checkpoints every 100 steps,
+    FP32 forward on the engine, FP64 adjoint.  The margin is raised to 40 A
+    so that the window holds no effective-domain rebuild (mdn_adjoint needs a
+    fixed molecule set)."""
+    from md_nucleation_b200 import generate
+    spec = generate.config1(0)
+    spec.margin = 40.0
+    with engine.Engine([spec]) as e:
+        e.step(10)
+        info = e.info(0)
+        window = 2000
+        if info.loop_update - info.loop_pair < window:
+            return {"unavailable": f"the next rebuild is {info.loop_update - info.loop_pair} steps away"}
+        J, grad, (fwd_ms, adj_ms) = e.adjoint(n_steps=window, checkpoint_every=100, count_radius=10.0,
+                                              count_width=1.0)
+        return {"cost_ratio": adj_ms / fwd_ms, "forward_ms": fwd_ms, "adjoint_ms": adj_ms, "n_params": len(grad),
+                "window_steps": window, "checkpoint_every": 100, "J": J,
+                "in_domain_atoms": int(info.n_ion + info.n_gas_in * spec.gas.n + info.n_vapor_in * spec.vapor.n),
+                "system": "150-atom +1 chain, 100 methanol, 100,000 rigid N2 (margin 40 A)"}
+
+
 def host_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -510,6 +534,9 @@ def run_engine(args):
     if rank == 0 and ws == 1 and not args.no_plain:
         pv, psample = plain_sample(engine, specs, checked, args.plain_replicas)
         out["plain"] = {"value": pv, "unit": UNIT, "sample": psample, "batched_over_plain": value / pv}
+    # the gradient harness's cost against its own forward window (rank 0, N = 1)
+    if rank == 0 and ws == 1 and not args.no_adjoint:
+        out["adjoint"] = adjoint_measurement(engine)
     # CPU baseline on rank 0 at N = 1 only
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         from oracle import bind
@@ -540,6 +567,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the one-system-per-launch measurement")
     ap.add_argument("--plain-replicas", type=int, default=16)
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the gradient-harness measurement")
     ap.add_argument("--cluster", type=int, default=0, help="CTAs per replica (1..8); 0 = tuned in the warm-up")
     args = ap.parse_args()
     if args.warmup < 3 and not os.environ.get("MDN_BENCH_ALLOW_SHORT"):

@@ -174,6 +174,12 @@ typedef struct mdn_replica_desc {
   double nvt_temperature;           /* Nose-Hoover target (pp->Tnh_ion) */
   double efield[3];                 /* Ecoeff for MDN_I_EFIELD */
   unsigned long long seed;          /* counter-based RNG key of this replica */
+  /* optional LJ parameters per type pair, [n_atom_types^2] row-major and
+   * symmetric, used instead of the Lorentz-Berthelot mixing of
+   * Variables::setCrossPotentials (src/initialization/setCrossPotential.cpp:4-23);
+   * NULL = mixing.  The parameters of the gradient harness (mdn_adjoint). */
+  const double* pair_eps;
+  const double* pair_sigma;
 } mdn_replica_desc;
 
 typedef struct mdn_options {
@@ -313,6 +319,48 @@ int  mdn_snapshot(mdn_handle* h, long long* offset, long long capacity, int* typ
 #define MDN_NOALLOC_MAX_REPLICAS 1024
 int  mdn_snapshot_noalloc(mdn_handle* h, long long* offset, long long capacity, int* type, double* x,
                           double* v, double* U);
+/* ---- gradient harness (no counterpart in the reference) -------------------
+ * Sensitivities of an ion-vapor objective over a window of MD steps of one
+ * replica to the gas-ion and vapor-ion LJ parameters and to a scale of the
+ * ion's charges.  The objective is
+ *   J = (1/n) sum_{t=1..n} [ w_energy * U_vi(x_t) + w_count * sum_m S(|c_m - c_ion|) ]
+ * with U_vi the ion-vapor LJ + Coulomb energy (PotentialVaporIon's Uvi,
+ * src/potential/VaporIon.cpp:5-43), c_m the centre of in-domain vapor
+ * molecule m, c_ion the ion centre and S(r) = 1 / (1 + exp((r - R0) / W))
+ * a smooth count of molecules within R0.  The parameters, in the order of
+ * mdn_adjoint_params: (eps, sigma) of every (gas type, ion type) pair of the
+ * replica, then of every (vapor type, ion type) pair, then the charge scale s
+ * (ion charges q -> s q, derivative taken at s = 1).
+ * The engine runs the window forward (FP32 pair terms) and keeps the
+ * replica state every `checkpoint_every` steps; the adjoint then walks the
+ * segments backwards, recomputing each one in FP64 from its checkpoint and
+ * running reverse velocity Verlet through it: transposed force Jacobians of
+ * the pair terms (with the taper weights and their dependence on the ion
+ * centre), Jacobian-vector products of the bonded terms, and the adjoint of
+ * the converged SHAKE projection with its velocity correction.  The window
+ * must hold no effective-domain rebuild (the molecule set is fixed): a
+ * window that would cross one is an error (raise Margin or shorten it).
+ * Needs a handle with one replica and the thermostat off.               */
+typedef struct mdn_adjoint_spec {
+  long long n_steps;        /* window length                                  */
+  int checkpoint_every;     /* K: steps per recomputed segment                */
+  double count_radius;      /* R0 (A)                                         */
+  double count_width;       /* W (A)                                          */
+  double w_energy;          /* weight of U_vi                                 */
+  double w_count;           /* weight of the smooth count                     */
+} mdn_adjoint_spec;
+/* Parameter rows of mdn_adjoint's gradient: rows[3*k] = 0 (gas-ion) / 1
+ * (vapor-ion) / 2 (charge scale), rows[3*k+1..2] = the two types; parameter
+ * 2k is the pair's eps, 2k+1 its sigma, the last one the charge scale.
+ * *n_params receives the count; rows may be NULL.                          */
+int  mdn_adjoint_params(const mdn_replica_desc* d, int* n_params, int* rows, int capacity);
+/* Runs the window from the replica's current state (it advances by n_steps)
+ * and returns J and dJ/dtheta (grad: n_params doubles).  d must be the
+ * descriptor the handle was created with.  ms (may be NULL) receives the
+ * device time of the forward window and of the adjoint (ms[0], ms[1]).     */
+int  mdn_adjoint(mdn_handle* h, const mdn_replica_desc* d, const mdn_adjoint_spec* spec, double* J,
+                 double* grad, double* ms);
+
 /* Page-locked host memory for mdn_snapshot / mdn_upload_state buffers. */
 int  mdn_host_alloc(size_t bytes, void** ptr);
 int  mdn_host_free(void* ptr);

@@ -76,6 +76,14 @@ class ReplicaDesc(C.Structure):
         ("cutoff", C.c_double), ("margin", C.c_double), ("r_inter", C.c_double), ("overlap", C.c_double),
         ("interactions", C.c_uint), ("nvt_mode", C.c_int), ("nvt_temperature", C.c_double),
         ("efield", C.c_double * 3), ("seed", C.c_ulonglong),
+        ("pair_eps", C.POINTER(C.c_double)), ("pair_sigma", C.POINTER(C.c_double)),
+    ]
+
+
+class AdjointSpec(C.Structure):
+    _fields_ = [
+        ("n_steps", C.c_longlong), ("checkpoint_every", C.c_int), ("count_radius", C.c_double),
+        ("count_width", C.c_double), ("w_energy", C.c_double), ("w_count", C.c_double),
     ]
 
 

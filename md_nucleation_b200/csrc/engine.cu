@@ -297,6 +297,8 @@ __attribute__((visibility("hidden"))) void mdn_snapshot_args(const mdn_handle* h
 
 __attribute__((visibility("hidden"))) int mdn_error(int code, const char* msg) { return fail(code, "%s", msg); }
 
+__attribute__((visibility("hidden"))) unsigned mdn_internal_quirks(const mdn_handle* h) { return h->opt.quirks; }
+
 extern "C" {
 
 int mdn_abi_version(void) { return MDN_ABI_VERSION; }
@@ -481,8 +483,8 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
       std::vector<double> A((size_t)nt * nt), B((size_t)nt * nt);
       for (int i = 0; i < nt; i++)
         for (int j = 0; j < nt; j++) {
-          double epu = sqrt(d.atom_eps[i] * d.atom_eps[j]);
-          double sigma = (d.atom_sigma[i] + d.atom_sigma[j]) * 0.5;
+          double epu = d.pair_eps ? d.pair_eps[(size_t)i * nt + j] : sqrt(d.atom_eps[i] * d.atom_eps[j]);
+          double sigma = d.pair_sigma ? d.pair_sigma[(size_t)i * nt + j] : (d.atom_sigma[i] + d.atom_sigma[j]) * 0.5;
           A[(size_t)i * nt + j] = 48 * epu * pow(sigma, 12.0);
           B[(size_t)i * nt + j] = 24 * epu * pow(sigma, 6.0);
         }

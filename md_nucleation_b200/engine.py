@@ -63,6 +63,9 @@ def lib():
         L.mdn_set_launch.argtypes = [vp, C.c_int, C.c_int, C.c_int]
         L.mdn_get_launch.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.mdn_tune_launch.argtypes = [vp, C.c_longlong, C.POINTER(C.c_int)]
+        L.mdn_adjoint_params.argtypes = [C.POINTER(abi.ReplicaDesc), C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int]
+        L.mdn_adjoint.argtypes = [vp, C.POINTER(abi.ReplicaDesc), C.POINTER(abi.AdjointSpec),
+                                  C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.mdn_snapshot.argtypes = [vp, C.POINTER(C.c_longlong), C.c_longlong, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.POINTER(C.c_double)]
         L.mdn_host_alloc.argtypes = [C.c_size_t, C.POINTER(C.c_void_p)]
@@ -210,6 +213,30 @@ class Engine:
         best = C.c_int(0)
         _ck(self.L.mdn_tune_launch(self.h, n_steps, C.byref(best)))
         return best.value
+
+    # ---- gradient harness ------------------------------------------------------
+    def adjoint_params(self):
+        """Rows (kind, type_a, type_b) of mdn_adjoint's gradient: kind 0 =
+        gas-ion pair (eps at 2k, sigma at 2k+1), 1 = vapor-ion pair, 2 = the
+        ion charge scale (the last parameter)."""
+        n = C.c_int(0)
+        _ck(self.L.mdn_adjoint_params(C.byref(self._descs[0]), C.byref(n), None, 0))
+        rows = np.zeros((n.value // 2 + 1, 3), np.int32)
+        _ck(self.L.mdn_adjoint_params(C.byref(self._descs[0]), C.byref(n), abi.ptr(rows, C.c_int), len(rows)))
+        return rows, n.value
+
+    def adjoint(self, n_steps: int, checkpoint_every: int = 100, count_radius: float = 10.0,
+                count_width: float = 1.0, w_energy: float = 1.0, w_count: float = 1.0):
+        """mdn_adjoint over the next n_steps of the (single) replica; returns
+        (J, dJ/dtheta, (forward ms, adjoint ms)).  The replica advances."""
+        spec = abi.AdjointSpec(n_steps, checkpoint_every, count_radius, count_width, w_energy, w_count)
+        _, n = self.adjoint_params()
+        J = C.c_double(0)
+        grad = np.zeros(n)
+        ms = np.zeros(2)
+        _ck(self.L.mdn_adjoint(self.h, C.byref(self._descs[0]), C.byref(spec), C.byref(J), abi.ptr(grad),
+                               abi.ptr(ms)))
+        return J.value, grad, (float(ms[0]), float(ms[1]))
 
     def set_launch(self, cluster_size=0, threads=0, steps_per_launch=-1):
         _ck(self.L.mdn_set_launch(self.h, cluster_size, threads, steps_per_launch))

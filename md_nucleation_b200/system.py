@@ -125,6 +125,10 @@ class ReplicaSpec:
     seed: int = 1
     pressure: float = 1e5
     label: str = ""
+    # optional per-type-pair LJ parameters [nt, nt] (symmetric) used instead
+    # of Lorentz-Berthelot mixing; None = mixing
+    pair_eps: Optional[np.ndarray] = None
+    pair_sigma: Optional[np.ndarray] = None
 
     def __post_init__(self):
         f64 = lambda a, s=None: np.ascontiguousarray(np.asarray(a, np.float64).reshape(s) if s else np.asarray(a, np.float64))
@@ -190,7 +194,21 @@ class ReplicaSpec:
         for k in range(3):
             d.efield[k] = float(self.efield[k])
         d.seed = int(self.seed) & 0xFFFFFFFFFFFFFFFF
+        if self.pair_eps is not None or self.pair_sigma is not None:
+            eps, sig = self.pair_parameters()
+            keep += [eps, sig]
+            d.pair_eps, d.pair_sigma = abi.ptr(eps), abi.ptr(sig)
         return d, keep
+
+    def pair_parameters(self):
+        """(eps, sigma) per type pair [nt, nt]: the overrides, else mixing."""
+        eps = np.sqrt(np.outer(self.atom_eps, self.atom_eps))
+        sig = 0.5 * (self.atom_sigma[:, None] + self.atom_sigma[None, :])
+        if self.pair_eps is not None:
+            eps = np.ascontiguousarray(self.pair_eps, np.float64)
+        if self.pair_sigma is not None:
+            sig = np.ascontiguousarray(self.pair_sigma, np.float64)
+        return np.ascontiguousarray(eps), np.ascontiguousarray(sig)
 
     # ---- derived quantities ------------------------------------------------
     def lj_table(self):

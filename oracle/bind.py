@@ -187,6 +187,10 @@ def orc_lib():
         L.orc_rotate.argtypes = [C.c_double] * 6 + [C.c_int, C.POINTER(C.c_double)]
         L.orc_philox.argtypes = [C.c_ulonglong, C.c_uint * 4, C.POINTER(C.c_uint)]
         L.orc_step_many.argtypes = [C.POINTER(vp), C.c_int, C.c_longlong, C.c_int]
+        L.orc_objective.restype = C.c_double
+        L.orc_objective.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_double]
+        L.orc_window.restype = C.c_double
+        L.orc_window.argtypes = [vp, C.c_longlong, C.c_double, C.c_double, C.c_double, C.c_double]
         _orc = L
     return _orc
 
@@ -280,6 +284,13 @@ class OracleReplica:
         out = np.zeros(4)
         self.L.orc_kinetic(self.h, abi.ptr(out))
         return out
+
+    def objective(self, R0=10.0, W=1.0, w_energy=1.0, w_count=1.0):
+        return self.L.orc_objective(self.h, R0, W, w_energy, w_count)
+
+    def window(self, n, R0=10.0, W=1.0, w_energy=1.0, w_count=1.0):
+        """Advances n steps; the window average of the objective."""
+        return self.L.orc_window(self.h, n, R0, W, w_energy, w_count)
 
 
 def orc_rotate(a, b, c, x, y, z, zy_quirk=0):

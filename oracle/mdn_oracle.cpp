@@ -891,6 +891,44 @@ struct Oracle {
     step++;
   }
 
+  /* The gradient harness's objective at the current state:
+   *   w_energy * U_vi + w_count * sum_m 1 / (1 + exp((|c_m - c_ion| - R0) / W))
+   * U_vi as PotentialVaporIon accumulates it (src/potential/VaporIon.cpp:5-43,
+   * unweighted), c_m the mass centre of in-domain vapor molecule m, c_ion the
+   * ion's mass centre of its atom positions. */
+  double objective(double R0, double W, double we, double wc) const {
+    double U = 0;
+    for (int q : vap_in)
+      for (int a = 0; a < a_v; a++) {
+        const V3& xa = vx[(size_t)q * a_v + a];
+        for (int j = 0; j < ion.n; j++) {
+          double dx = xa[0] - ion_x[j][0], dy = xa[1] - ion_x[j][1], dz = xa[2] - ion_x[j][2];
+          double r2 = dx * dx + dy * dy + dz * dz;
+          double r2inv = 1 / r2;
+          double r6inv = r2inv * r2inv * r2inv;
+          int ta = vap.type[a], tj = ion.type[j];
+          U += r6inv * (A(ta, tj) / 12.0 * r6inv - B(ta, tj) / 6.0) + qqrd2e * vap.q[a] * ion.q[j] * sqrt(r2inv);
+        }
+      }
+    V3 c = {0, 0, 0};
+    for (int j = 0; j < ion.n; j++)
+      for (int k = 0; k < 3; k++) c[k] += ion_x[j][k] * ion.mass[j];
+    for (int k = 0; k < 3; k++) c[k] /= ion.msum;
+    double S = 0;
+    for (int q : vap_in) {
+      V3 cm = {0, 0, 0};
+      for (int a = 0; a < a_v; a++)
+        for (int k = 0; k < 3; k++) cm[k] += vx[(size_t)q * a_v + a][k] * vap.mass[a];
+      double d2 = 0;
+      for (int k = 0; k < 3; k++) {
+        double dk = cm[k] / vap.msum - c[k];
+        d2 += dk * dk;
+      }
+      S += 1.0 / (1.0 + exp((sqrt(d2) - R0) / W));
+    }
+    return we * U + wc * S;
+  }
+
   void build_exclusions() {
     excl.assign((size_t)ion.n * ion.n, 0);
     auto mark = [&](int i, int j) {
@@ -914,8 +952,8 @@ Oracle* create(const mdn_replica_desc* d, unsigned quirks, int force_mode) {
   o->ljB.resize((size_t)o->nt * o->nt);
   for (int i = 0; i < o->nt; i++)
     for (int j = 0; j < o->nt; j++) {
-      double epu = sqrt(d->atom_eps[i] * d->atom_eps[j]);
-      double sigma = (d->atom_sigma[i] + d->atom_sigma[j]) * 0.5;
+      double epu = d->pair_eps ? d->pair_eps[(size_t)i * o->nt + j] : sqrt(d->atom_eps[i] * d->atom_eps[j]);
+      double sigma = d->pair_sigma ? d->pair_sigma[(size_t)i * o->nt + j] : (d->atom_sigma[i] + d->atom_sigma[j]) * 0.5;
       o->ljA[(size_t)i * o->nt + j] = 48 * epu * pow(sigma, 12.0);
       o->ljB[(size_t)i * o->nt + j] = 24 * epu * pow(sigma, 6.0);
     }
@@ -1147,6 +1185,25 @@ int orc_pair_list(void* h, int kind, int* pairs, int capacity) {
 }
 
 /* Kion, Kgas, Kvap, Tion (Observer::computeProps) */
+/* The gradient harness's objective at the current state (Oracle::objective). */
+double orc_objective(void* h, double R0, double W, double we, double wc) {
+  return ((Oracle*)h)->objective(R0, W, we, wc);
+}
+
+/* Advances n steps and returns the window average of the objective after
+ * each step: the quantity mdn_adjoint differentiates. */
+double orc_window(void* h, long long n, double R0, double W, double we, double wc) {
+  Oracle* o = (Oracle*)h;
+  double s = 0;
+  for (int k = 0; k < 8; k++) o->U[k] = 0;
+  for (long long t = 0; t < n; t++) {
+    o->eflag = 0;
+    o->verlet();
+    s += o->objective(R0, W, we, wc);
+  }
+  return n > 0 ? s / (double)n : 0.0;
+}
+
 void orc_kinetic(void* h, double* out) {
   Oracle* o = (Oracle*)h;
   double Kg = 0, Kv = 0;

@@ -84,6 +84,11 @@ extern "C" {
 /* Builds a replica.  do_make_pair = 1 performs the initial MD::make_pair of
  * MD::MD; 0 leaves every molecule outside the domain. */
 void* ref_create(const mdn_replica_desc* d, int do_make_pair) {
+  /* the reference mixes LJ parameters itself (Variables::setCrossPotentials) */
+  if (d->pair_eps || d->pair_sigma) {
+    fprintf(stderr, "ref_create: per-pair LJ parameters have no counterpart in the reference\n");
+    return nullptr;
+  }
   Harness* h = new Harness();
   MD* md = new MD(nullptr, 0);
   h->md = md;
