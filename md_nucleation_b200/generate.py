@@ -236,7 +236,12 @@ def chain(n_atoms: int, charge: float, rng: np.random.Generator) -> Species:
         np.fill_diagonal(bad, False)
         return not bad.any()
 
-    for _attempt in range(400):
+    for _attempt in range(800):
+        # heavy atoms three or more bonds apart stay 3.6 A apart; after 400
+        # failed attempts (long chains, whose near-trans walks jam) the 1-4
+        # neighbours, excluded from the non-bonded terms anyway, only need
+        # 3.0 A (gauche or trans, not cis)
+        skip = 2 if _attempt < 400 else 3
         bb = [np.zeros(3)]
         bl = rng.uniform(1.33, 1.53, n_heavy)
         ok = True
@@ -252,7 +257,8 @@ def chain(n_atoms: int, charge: float, rng: np.random.Generator) -> Species:
                     perp = _perp(prev, rng)
                     d = math.cos(math.pi - th) * prev + math.sin(math.pi - th) * perp
                 cand = bb[-1] + bl[i] * d
-                if all(np.linalg.norm(cand - p_) > 3.6 for p_ in bb[:-2]):
+                if all(np.linalg.norm(cand - p_) > 3.6 for p_ in bb[:-skip]) and (
+                        skip == 2 or len(bb) < 3 or np.linalg.norm(cand - bb[-3]) > 3.0):
                     bb.append(cand)
                     break
             else:
