@@ -596,6 +596,44 @@ __device__ __forceinline__ float born(float r2, int ti, int tj, float qq, float*
   return (f1 + f2 + f3 + fc) * r2inv;
 }
 
+/* FP64 forms of the pair terms (mdn_options.force_mode = 1), with the
+ * reference's FP64 constants (src/potential/BMHFT/potentialBMHFT.hpp:21-39) */
+__constant__ double kBornD[2][2][5] = {
+    {{25.4435 * 3.1546 / 4.184, 6. * 101.1719 / 4.184, 8. * 48.1771 / 4.184, 2.340, 3.1546},
+     {20.3548 * 3.1546 / 4.184, 6. * 674.4793 / 4.184, 8. * 837.077 / 4.184, 2.755, 3.1546}},
+    {{20.3548 * 3.1546 / 4.184, 6. * 674.4793 / 4.184, 8. * 837.077 / 4.184, 2.755, 3.1546},
+     {15.2661 * 3.1546 / 4.184, 6. * 6985.6786 / 4.184, 8. * 14031.5785 / 4.184, 3.170, 3.1546}}};
+
+__device__ __forceinline__ double lj_coul_d(double r2, double A, double B, double qq, bool coul) {
+  double r2inv = 1 / r2;
+  double r6inv = r2inv * r2inv * r2inv;
+  double f = r6inv * (A * r6inv - B);
+  if (coul) f += qq * sqrt(r2inv);
+  return f * r2inv;
+}
+
+__device__ __forceinline__ double born_d(double r2, int ti, int tj, double qq) {
+  const double* c = kBornD[ti][tj];
+  double r2inv = 1 / r2;
+  double r6inv = r2inv * r2inv * r2inv;
+  double r = sqrt(r2);
+  double rexp = exp(c[4] * (c[3] - r));
+  return (c[4] * c[0] * r * rexp - c[1] * r6inv - c[2] * r6inv * r2inv + qq * sqrt(r2inv)) * r2inv;
+}
+
+/* taper weight of core atom i in FP64: the float copy is exact at 0 and 1 */
+__device__ __forceinline__ double weight_d(const Ctx& x, int i) {
+  const float w = x.c.w[i];
+  if (w == 0.0f || w == 1.0f) return (double)w;
+  return taper(x.P, x.D->ion_com, x.c.x + 3 * i);
+}
+
+/* charge of core atom i */
+__device__ __forceinline__ double charge_d(const Ctx& x, int i) {
+  const RepParams* P = x.P;
+  return i < P->n_ion ? x.db[P->d_ion_q + i] : x.db[P->d_vap_q + (i - P->n_ion) % P->a_v];
+}
+
 /* ------------------------------------------------------------------------- */
 /* forces of the core (ion + vapor) among themselves, and the core kick        */
 /* ------------------------------------------------------------------------- */
@@ -619,7 +657,8 @@ __device__ __forceinline__ bool term_on(const Ctx& x, unsigned bit) {
  * ordered pair (i, j) is evaluated on i's side (the full matrix): the i force
  * stays in registers and reaches the core sums once per tile, with no
  * reaction atomics; energies count each pair once (j > i). */
-__device__ void core_pairs(Ctx& x, bool eflag) {
+template <bool FP64>
+__device__ void core_pairs_t(Ctx& x, bool eflag) {
   const RepParams* P = x.P;
   const int ni = P->n_ion, nc = x.n_core, nt = P->n_types;
   const bool amber = term_on(x, MDN_I_AMBER), bmh = term_on(x, MDN_I_BMH);
@@ -642,6 +681,12 @@ __device__ void core_pairs(Ctx& x, bool eflag) {
     const float wi = x.c.w[ii];
     const bool iion = ii < ni;
     const int bi = (bmh && iion) ? bmht[ii] : 0;
+    double xd[3], wid = 1.0, qid = 0.0;
+    if constexpr (FP64) {
+      for (int k = 0; k < 3; k++) xd[k] = x.c.x[3 * ii + k];
+      wid = weight_d(x, ii);
+      qid = charge_d(x, ii);
+    }
     long long F0 = 0, F1 = 0, F2 = 0;
     const int j0 = jb * 32, j1 = min(nc, j0 + 32);
     for (int j = j0; j < j1; j++) {
@@ -684,9 +729,27 @@ __device__ void core_pairs(Ctx& x, bool eflag) {
         }
       }
       if (!any) continue;
-      F0 += fixf(fp * dx);
-      F1 += fixf(fp * dy);
-      F2 += fixf(fp * dz);
+      if constexpr (FP64) {
+        /* the same terms in FP64 from the FP64 positions and tables */
+        const double ex = xd[0] - x.c.x[3 * j], ey = xd[1] - x.c.x[3 * j + 1], ez = xd[2] - x.c.x[3 * j + 2];
+        const double R2 = ex * ex + ey * ey + ez * ez;
+        const double qq = P->qqrd2e * qid * charge_d(x, j);
+        const double Ad = x.db[P->d_ljA + ti * nt + tj], Bd = x.db[P->d_ljB + ti * nt + tj];
+        double fd = 0.0;
+        if (bucket == 1) {
+          if (amber && !((x.c.excl[i * P->excl_words + (j >> 5)] >> (j & 31)) & 1u)) fd += lj_coul_d(R2, Ad, Bd, qq, true);
+          if (bmh) fd += born_d(R2, bi, bmht[j], qq);
+        } else {
+          fd = lj_coul_d(R2, Ad, Bd, qq, true) * (wid * weight_d(x, j));
+        }
+        F0 += fixd(fd * ex);
+        F1 += fixd(fd * ey);
+        F2 += fixd(fd * ez);
+      } else {
+        F0 += fixf(fp * dx);
+        F1 += fixf(fp * dy);
+        F2 += fixf(fp * dz);
+      }
       if (eflag && j > i) {
         const double R2 = r2d(x.c.x + 3 * i, x.c.x + 3 * j);
         const double qi = i < ni ? x.db[P->d_ion_q + i] : x.db[P->d_vap_q + (i - ni) % P->a_v];
@@ -721,6 +784,18 @@ __device__ void core_pairs(Ctx& x, bool eflag) {
     }
   }
 }
+
+/* MDN_FP64_PAIRS selects the pair precision of this compilation: the FP64
+ * form (mdn_options.force_mode = 1) is compiled into its own kernel,
+ * mdn_advance_fp64 (advance_fp64.cu), so that the FP32 kernel's registers
+ * and code are not shaped by it */
+#ifdef MDN_FP64_PAIRS
+constexpr bool kFP64Pairs = true;
+#else
+constexpr bool kFP64Pairs = false;
+#endif
+
+__device__ void core_pairs(Ctx& x, bool eflag) { core_pairs_t<kFP64Pairs>(x, eflag); }
 
 __device__ void core_bonded(Ctx& x, bool eflag) {
   const RepParams* P = x.P;
@@ -987,7 +1062,7 @@ __device__ void gas_far_pass(Ctx& x, bool eflag, bool kick) {
  * batched workload, so a wider split leaves lanes idle); the molecule's own
  * force stays in registers, the reaction goes to the core sums by shared
  * 64-bit integer atomics, so the result does not depend on the order */
-template <int AG>
+template <int AG, bool FP64>
 __device__ void gas_near_pass_t(Ctx& x, bool eflag, bool kick) {
   const RepParams* P = x.P;
   const KArgs* a = x.a;
@@ -1042,11 +1117,20 @@ __device__ void gas_near_pass_t(Ctx& x, bool eflag, bool kick) {
         int tj = x.c.type[j];
         long long R[3] = {0, 0, 0};
         for (int at = 0; at < ag; at++) {
-          float dx = gp[at].x - pj.x, dy = gp[at].y - pj.y, dz = gp[at].z - pj.z;
-          float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-          float ee;
-          float fp = lj_coul(r2, x.c.ljA[gtype[at] * nt + tj], x.c.ljB[gtype[at] * nt + tj], 0.0f, false, &ee);
-          long long fx = fixf(fp * dx), fy = fixf(fp * dy), fz = fixf(fp * dz);
+          long long fx, fy, fz;
+          if constexpr (FP64) {
+            const double ex = X[3 * at] - x.c.x[3 * j], ey = X[3 * at + 1] - x.c.x[3 * j + 1],
+                         ez = X[3 * at + 2] - x.c.x[3 * j + 2];
+            const double fd = lj_coul_d(ex * ex + ey * ey + ez * ez, x.db[P->d_ljA + gtype[at] * nt + tj],
+                                        x.db[P->d_ljB + gtype[at] * nt + tj], 0.0, false);
+            fx = fixd(fd * ex); fy = fixd(fd * ey); fz = fixd(fd * ez);
+          } else {
+            float dx = gp[at].x - pj.x, dy = gp[at].y - pj.y, dz = gp[at].z - pj.z;
+            float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            float ee;
+            float fp = lj_coul(r2, x.c.ljA[gtype[at] * nt + tj], x.c.ljB[gtype[at] * nt + tj], 0.0f, false, &ee);
+            fx = fixf(fp * dx); fy = fixf(fp * dy); fz = fixf(fp * dz);
+          }
           F[at][0] += fx; F[at][1] += fy; F[at][2] += fz;
           R[0] -= fx; R[1] -= fy; R[2] -= fz;
           if (eflag)
@@ -1066,11 +1150,20 @@ __device__ void gas_near_pass_t(Ctx& x, bool eflag, bool kick) {
           int tj = x.c.type[j];
           long long R[3] = {0, 0, 0};
           for (int at = 0; at < ag; at++) {
-            float dx = gp[at].x - pj.x, dy = gp[at].y - pj.y, dz = gp[at].z - pj.z;
-            float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            float ee;
-            float fp = lj_coul(r2, x.c.ljA[gtype[at] * nt + tj], x.c.ljB[gtype[at] * nt + tj], 0.0f, false, &ee);
-            long long fx = fixf(fp * dx), fy = fixf(fp * dy), fz = fixf(fp * dz);
+            long long fx, fy, fz;
+            if constexpr (FP64) {
+              const double ex = X[3 * at] - x.c.x[3 * j], ey = X[3 * at + 1] - x.c.x[3 * j + 1],
+                           ez = X[3 * at + 2] - x.c.x[3 * j + 2];
+              const double fd = lj_coul_d(ex * ex + ey * ey + ez * ez, x.db[P->d_ljA + gtype[at] * nt + tj],
+                                          x.db[P->d_ljB + gtype[at] * nt + tj], 0.0, false);
+              fx = fixd(fd * ex); fy = fixd(fd * ey); fz = fixd(fd * ez);
+            } else {
+              float dx = gp[at].x - pj.x, dy = gp[at].y - pj.y, dz = gp[at].z - pj.z;
+              float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+              float ee;
+              float fp = lj_coul(r2, x.c.ljA[gtype[at] * nt + tj], x.c.ljB[gtype[at] * nt + tj], 0.0f, false, &ee);
+              fx = fixf(fp * dx); fy = fixf(fp * dy); fz = fixf(fp * dz);
+            }
             F[at][0] += fx; F[at][1] += fy; F[at][2] += fz;
             R[0] -= fx; R[1] -= fy; R[2] -= fz;
             if (eflag)
@@ -1113,8 +1206,8 @@ __device__ void gas_near_pass_t(Ctx& x, bool eflag, bool kick) {
 }
 
 __device__ void gas_near_pass(Ctx& x, bool eflag, bool kick) {
-  if (x.P->a_g == 1) gas_near_pass_t<1>(x, eflag, kick);
-  else gas_near_pass_t<2>(x, eflag, kick);
+  if (x.P->a_g == 1) gas_near_pass_t<1, kFP64Pairs>(x, eflag, kick);
+  else gas_near_pass_t<2, kFP64Pairs>(x, eflag, kick);
 }
 
 /* sum of the core partials over the cluster -> f (double), identical in every CTA */
@@ -1829,7 +1922,12 @@ __device__ void one_step(Ctx& x, cg::cluster_group& cl, bool eflag) {
 
 }  // namespace
 
-extern "C" __global__ void __launch_bounds__(512, 1) mdn_advance(KArgs a) {
+#ifdef MDN_FP64_PAIRS
+#define MDN_ADVANCE_KERNEL mdn_advance_fp64
+#else
+#define MDN_ADVANCE_KERNEL mdn_advance
+#endif
+extern "C" __global__ void __launch_bounds__(512, 1) MDN_ADVANCE_KERNEL(KArgs a) {
   cg::cluster_group cl = cg::this_cluster();
   extern __shared__ __align__(16) unsigned char dsm[];
   __shared__ RepParams sP;

@@ -25,6 +25,7 @@
 #include "mdn_types.h"
 
 extern "C" __global__ void mdn_advance(KArgs a);
+extern "C" __global__ void mdn_advance_fp64(KArgs a);
 int mdn_snapshot_device(const RepParams* dP, const RepDyn* dD, const int* d_iblob, int R, const double* ion_x,
                         const double* ion_v, const double* slab_x, const double* slab_v, const double* vslab_x,
                         const double* vslab_v, long long* d_offset, int* d_type, double* d_x, double* d_v,
@@ -261,7 +262,7 @@ long long launch(mdn_handle* h, int mode, long long n_steps, int energy_mode, un
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  e = cudaLaunchKernelEx(&cfg, mdn_advance, a);
+  e = cudaLaunchKernelEx(&cfg, h->opt.force_mode ? mdn_advance_fp64 : mdn_advance, a);
   if (e != cudaSuccess) {
     *rc = fail(MDN_ERR_CUDA, "kernel launch: %s", cudaGetErrorString(e));
     return 0;
@@ -672,8 +673,10 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
   ck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
   ck(cudaEventCreate(&h->ev0), "event");
   ck(cudaEventCreate(&h->ev1), "event");
-  ck(cudaFuncSetAttribute(mdn_advance, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem), "smem attr");
-  ck(cudaFuncSetAttribute(mdn_advance, cudaFuncAttributeNonPortableClusterSizeAllowed, 1), "cluster attr");
+  for (auto kern : {mdn_advance, mdn_advance_fp64}) {
+    ck(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem), "smem attr");
+    ck(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1), "cluster attr");
+  }
   ck(cudaMemcpy(h->dP, h->P.data(), sizeof(RepParams) * R, cudaMemcpyHostToDevice), "params");
   ck(cudaMemcpy(h->dD, h->D0.data(), sizeof(RepDyn) * R, cudaMemcpyHostToDevice), "dyn");
   ck(cudaMemcpy(h->d_iblob, iblob.data(), sizeof(int) * iblob.size(), cudaMemcpyHostToDevice), "iblob");

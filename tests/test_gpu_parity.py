@@ -76,6 +76,23 @@ def test_forces_match_fp64_oracle(eng, oracle_libs, name, term):
     assert np.all(np.abs(Ue - Uo) <= 1e-4 * scale + 1e-6), f"energies {Ue} vs {Uo}"
 
 
+@pytest.mark.parametrize("name", NAMES)
+def test_fp64_pair_mode_forces(eng, oracle_libs, name):
+    """force_mode 1: the pair terms in FP64 (64-bit fixed-point sums of
+    2^-40 kcal/mol/A quanta) agree with the FP64 oracle within 1e-9."""
+    spec = systems.make(name)
+    o = oracle_libs.OracleReplica(spec)
+    o.step(3)
+    st = o.get_state()
+    e = eng.Engine([spec], force_mode=1)
+    e.upload(0, st)
+    o.set_state(st)
+    e.compute_forces(0)
+    o.compute_forces(0)
+    err = rel_rms(forces_of(e.state(0), spec), forces_of(o.get_state(), spec))
+    assert err <= 1e-9, f"relative RMS force error {err:.2e}"
+
+
 @pytest.mark.parametrize("quirks", INSERTION)
 @pytest.mark.parametrize("name", NAMES)
 def test_trajectory_across_rebuild(eng, oracle_libs, name, quirks):
