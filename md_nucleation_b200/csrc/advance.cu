@@ -210,50 +210,25 @@ __device__ double ion_temperature(Ctx& x) {
   return T;
 }
 
-/* residual |s^2 - d^2| of constraint k */
-__device__ __forceinline__ double shake_residual(const double* X, int i, int j, double dk) {
-  double sx = X[3 * i] - X[3 * j], sy = X[3 * i + 1] - X[3 * j + 1], sz = X[3 * i + 2] - X[3 * j + 2];
-  double dr = sx * sx + sy * sy + sz * sz - dk * dk;
-  return dr * dr;
-}
-
-/* one SHAKE correction of constraint (i, j) with reference vector R_i - R_j */
-__device__ __forceinline__ void shake_pair(double* X, const double* R, int i, int j, double dk, double mi, double mj) {
-  double rx = R[3 * i] - R[3 * j], ry = R[3 * i + 1] - R[3 * j + 1], rz = R[3 * i + 2] - R[3 * j + 2];
-  double sx = X[3 * i] - X[3 * j], sy = X[3 * i + 1] - X[3 * j + 1], sz = X[3 * i + 2] - X[3 * j + 2];
-  double s2 = sx * sx + sy * sy + sz * sz;
-  double dot = rx * sx + ry * sy + rz * sz;
-  double minv = 1 / mi + 1 / mj;
+/* one SHAKE correction with the constraint's table row c = (d^2, 1/m_i,
+ * 1/m_j): the multiplier of shake_pair with one division */
+__device__ __forceinline__ void shake_pair_c(double* Xi, double* Xj, const double* Ri, const double* Rj,
+                                             const double* c) {
+  double r0 = Ri[0] - Rj[0], r1 = Ri[1] - Rj[1], r2 = Ri[2] - Rj[2];
+  double s0 = Xi[0] - Xj[0], s1 = Xi[1] - Xj[1], s2 = Xi[2] - Xj[2];
+  double ss = s0 * s0 + s1 * s1 + s2 * s2;
+  double dot = r0 * s0 + r1 * s1 + r2 * s2;
   if (dot < 1e-10) dot = 1e-10;
-  double g = (dk * dk - s2) / (2 * minv * dot);
-  double ci = g / mi, cj = g / mj;
-  X[3 * i] += rx * ci; X[3 * i + 1] += ry * ci; X[3 * i + 2] += rz * ci;
-  X[3 * j] -= rx * cj; X[3 * j + 1] -= ry * cj; X[3 * j + 2] -= rz * cj;
+  double g = (c[0] - ss) / (2 * (c[1] + c[2]) * dot);
+  double gi = g * c[1], gj = g * c[2];
+  Xi[0] += r0 * gi; Xi[1] += r1 * gi; Xi[2] += r2 * gi;
+  Xj[0] -= r0 * gj; Xj[1] -= r1 * gj; Xj[2] -= r2 * gj;
 }
 
-/* SHAKE of one small molecule by one thread (vapor, gas): sweeps in colour
- * order until every constraint satisfies (s^2 - d^2)^2 <= 1e-20 after a sweep */
-__device__ int shake_small(const Ctx& x, double* X, double* V, const double* R, const double* m, int n,
-                           const int* rigid, int n_rigid, const int* color, int n_colors, bool vcorr) {
-  const RepParams* P = x.P;
-  double X0[3 * MDN_MAX_VAP_ATOMS];
-  for (int q = 0; q < 3 * n; q++) X0[q] = X[q];
-  bool converge = false;
-  for (int sweep = 0; sweep < MDN_SHAKE_MAX_SWEEPS && !converge; sweep++) {
-    for (int c = 0; c < n_colors; c++)
-      for (int k = 0; k < n_rigid; k++) {
-        if (color[k] != c) continue;
-        int i = rigid[3 * k], j = rigid[3 * k + 1];
-        shake_pair(X, R, i, j, x.db[P->d_bond + 2 * rigid[3 * k + 2] + 1], m[i], m[j]);
-      }
-    converge = true;
-    for (int k = 0; k < n_rigid; k++)
-      if (shake_residual(X, rigid[3 * k], rigid[3 * k + 1], x.db[P->d_bond + 2 * rigid[3 * k + 2] + 1]) > 1e-20)
-        converge = false;
-  }
-  if (vcorr)
-    for (int q = 0; q < 3 * n; q++) V[q] += (X[q] - X0[q]) / P->dt;
-  return converge ? 0 : MDN_ST_SHAKE_NOCONV;
+__device__ __forceinline__ double shake_res_c(const double* Xi, const double* Xj, const double* c) {
+  double s0 = Xi[0] - Xj[0], s1 = Xi[1] - Xj[1], s2 = Xi[2] - Xj[2];
+  double dr = s0 * s0 + s1 * s1 + s2 * s2 - c[0];
+  return dr * dr;
 }
 
 __device__ void core_drift_shake(Ctx& x) {
@@ -285,15 +260,14 @@ __device__ void core_drift_shake(Ctx& x) {
         for (int k = threadIdx.x; k < P->n_ion_rigid; k += blockDim.x) {
           if (col[k] != c) continue;
           int i = rig[3 * k], j = rig[3 * k + 1];
-          shake_pair(x.c.x, xold, i, j, x.db[P->d_bond + 2 * rig[3 * k + 2] + 1],
-                     x.db[P->d_mass + x.c.type[i]], x.db[P->d_mass + x.c.type[j]]);
+          shake_pair_c(x.c.x + 3 * i, x.c.x + 3 * j, xold + 3 * i, xold + 3 * j, x.db + P->d_ion_cons + 3 * k);
         }
         __syncthreads();
       }
       if (threadIdx.x == 0) x.iscr[50] = 1;
       __syncthreads();
       for (int k = threadIdx.x; k < P->n_ion_rigid; k += blockDim.x)
-        if (shake_residual(x.c.x, rig[3 * k], rig[3 * k + 1], x.db[P->d_bond + 2 * rig[3 * k + 2] + 1]) > 1e-20)
+        if (shake_res_c(x.c.x + 3 * rig[3 * k], x.c.x + 3 * rig[3 * k + 1], x.db + P->d_ion_cons + 3 * k) > 1e-20)
           x.iscr[50] = 0;
       __syncthreads();
       int conv = x.iscr[50];
@@ -313,29 +287,35 @@ __device__ void core_drift_shake(Ctx& x) {
         }
     __syncthreads();
   }
-  /* vapor molecules: one thread each */
+  /* vapor molecules: one thread each, in place in shared memory, sweeps in
+   * colour order until every constraint holds after a sweep */
   if (P->n_vap_rigid > 0) {
-    const int av = P->a_v;
+    const int av = P->a_v, nr = P->n_vap_rigid, nco = P->n_vap_colors;
+    const int* rig = x.ib + P->o_vap_rigid;
+    const int* col = x.ib + P->o_vap_color;
+    const double* ct = x.db + P->d_vap_cons;
     for (int s = threadIdx.x; s < x.D->n_vap_in; s += blockDim.x) {
-      int base = P->n_ion + s * av;
-      double X[3 * MDN_MAX_VAP_ATOMS], V[3 * MDN_MAX_VAP_ATOMS], R[3 * MDN_MAX_VAP_ATOMS], m[MDN_MAX_VAP_ATOMS];
-      double Xd[3 * MDN_MAX_VAP_ATOMS];
-      for (int at = 0; at < av; at++) {
-        m[at] = x.db[P->d_mass + x.c.type[base + at]];
-        for (int k = 0; k < 3; k++) {
-          X[3 * at + k] = x.c.x[3 * (base + at) + k];
-          V[3 * at + k] = x.c.v[3 * (base + at) + k];
-          R[3 * at + k] = xold[3 * (base + at) + k];
-          Xd[3 * at + k] = X[3 * at + k];
-        }
+      const int base = P->n_ion + s * av;
+      double* X = x.c.x + 3 * base;
+      const double* R = xold + 3 * base;
+      bool conv = false;
+      for (int sweep = 0; sweep < MDN_SHAKE_MAX_SWEEPS && !conv; sweep++) {
+        for (int c = 0; c < nco; c++)
+          for (int k = 0; k < nr; k++) {
+            if (col[k] != c) continue;
+            const int i = rig[3 * k], j = rig[3 * k + 1];
+            shake_pair_c(X + 3 * i, X + 3 * j, R + 3 * i, R + 3 * j, ct + 3 * k);
+          }
+        conv = true;
+        for (int k = 0; k < nr; k++)
+          if (shake_res_c(X + 3 * rig[3 * k], X + 3 * rig[3 * k + 1], ct + 3 * k) > 1e-20) conv = false;
       }
-      int st = shake_small(x, X, V, R, m, av, x.ib + P->o_vap_rigid, P->n_vap_rigid, x.ib + P->o_vap_color,
-                           P->n_vap_colors, false);
-      if (st && x.rank == 0) set_status(x, st);
-      for (int at = 0; at < av; at++)
-        for (int k = 0; k < 3; k++) {
-          x.c.x[3 * (base + at) + k] = X[3 * at + k];
-          if (vcorr) x.c.v[3 * (base + at) + k] += (X[3 * at + k] - Xd[3 * at + k]) / P->dt;
+      if (!conv && x.rank == 0) set_status(x, MDN_ST_SHAKE_NOCONV);
+      if (vcorr)
+        for (int q = 0; q < 3 * av; q++) {
+          /* displacement by the constraints = x - (xold + v*dt) */
+          const double xd = R[q] + x.c.v[3 * base + q] * dt;
+          x.c.v[3 * base + q] += (X[q] - xd) / dt;
         }
     }
   }
@@ -652,11 +632,14 @@ __device__ __forceinline__ bool term_on(const Ctx& x, unsigned bit) {
   return (x.P->interactions & bit) && (!x.a->term_mask || (x.a->term_mask & bit));
 }
 
-/* Core pairs as tiles of 32 i atoms (one per lane) x 32 j atoms walked by
- * the whole warp, so every j load is a shared-memory broadcast.  Every
- * ordered pair (i, j) is evaluated on i's side (the full matrix): the i force
- * stays in registers and reaches the core sums once per tile, with no
- * reaction atomics; energies count each pair once (j > i). */
+/* Core pairs as 32 x 32 tiles (i block ib <= j block jb), one warp each,
+ * every unordered pair evaluated once.  Lane l owns atom i = 32 ib + l; at
+ * step s it pairs with j = 32 jb + ((l + s) mod 32), so the lanes read 32
+ * distinct j (no bank conflicts), and it keeps the reaction on that j in a
+ * register that moves one lane down after every step: after 32 steps lane l
+ * holds the whole reaction on j = 32 jb + l.  Diagonal tiles take steps
+ * 1..15 and half of step 16.  Both sides reach the core sums once per tile
+ * as 64-bit integers, so the result does not depend on the launch shape. */
 template <bool FP64>
 __device__ void core_pairs_t(Ctx& x, bool eflag) {
   const RepParams* P = x.P;
@@ -666,13 +649,19 @@ __device__ void core_pairs_t(Ctx& x, bool eflag) {
   if (!(amber || bmh || vi || vv)) return;
   const float qqf = (float)P->qqrd2e;
   const int nblk = (nc + 31) >> 5;
-  const int items = nblk * nblk;
+  const int tiles = nblk * (nblk + 1) / 2;
   const int lane = threadIdx.x & 31;
   const int nwb = blockDim.x >> 5;
   const int* bmht = x.ib + P->o_ion_bmh;
   long long e_ion = 0, e_vi = 0, e_vv = 0;
-  for (int it = x.rank * nwb + (threadIdx.x >> 5); it < items; it += x.C * nwb) {
-    const int ib = it / nblk, jb = it - ib * nblk;
+  for (int t = x.rank * nwb + (threadIdx.x >> 5); t < tiles; t += x.C * nwb) {
+    int ib = 0, rem = t;
+    while (rem >= nblk - ib) {
+      rem -= nblk - ib;
+      ib++;
+    }
+    const int jb = ib + rem;
+    const bool diag = ib == jb;
     const int i = ib * 32 + lane;
     const bool act = i < nc;
     const int ii = act ? i : 0;
@@ -681,96 +670,112 @@ __device__ void core_pairs_t(Ctx& x, bool eflag) {
     const float wi = x.c.w[ii];
     const bool iion = ii < ni;
     const int bi = (bmh && iion) ? bmht[ii] : 0;
-    double xd[3], wid = 1.0, qid = 0.0;
+    double xd[3] = {0, 0, 0}, wid = 1.0, qid = 0.0;
     if constexpr (FP64) {
       for (int k = 0; k < 3; k++) xd[k] = x.c.x[3 * ii + k];
       wid = weight_d(x, ii);
       qid = charge_d(x, ii);
     }
-    long long F0 = 0, F1 = 0, F2 = 0;
-    const int j0 = jb * 32, j1 = min(nc, j0 + 32);
-    for (int j = j0; j < j1; j++) {
-      const float4 pj = x.c.pos[j];
-      const int tj = x.c.type[j], mj = x.c.mol[j];
-      const float wj = x.c.w[j];
-      if (!act || j == i) continue;
-      const bool jion = j < ni;
-      const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      float fp = 0.0f;
-      bool any = false;
-      int bucket = 0;
-      if (iion && jion) {
-        const bool ex = amber && ((x.c.excl[i * P->excl_words + (j >> 5)] >> (j & 31)) & 1u);
-        if (amber && !ex) {
-          float ee;
-          fp += lj_coul(r2, x.c.ljA[ti * nt + tj], x.c.ljB[ti * nt + tj], qqf * pi.w * pj.w, true, &ee);
-          any = true;
+    long long F0 = 0, F1 = 0, F2 = 0, R0 = 0, R1 = 0, R2 = 0;
+    for (int s = 0; s < 32; s++) {
+      const int j = jb * 32 + ((lane + s) & 31);
+      bool take = act && j < nc;
+      if (diag) take = take && s != 0 && (s < 16 || (s == 16 && lane < 16));
+      if (take) {
+        const float4 pj = x.c.pos[j];
+        const int tj = x.c.type[j], mj = x.c.mol[j];
+        const float wj = x.c.w[j];
+        const bool jion = j < ni;
+        const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        float fp = 0.0f;
+        bool any = false;
+        int bucket = 0;
+        if (iion && jion) {
+          const bool ex = amber && ((x.c.excl[i * P->excl_words + (j >> 5)] >> (j & 31)) & 1u);
+          if (amber && !ex) {
+            float ee;
+            fp += lj_coul(r2, x.c.ljA[ti * nt + tj], x.c.ljB[ti * nt + tj], qqf * pi.w * pj.w, true, &ee);
+            any = true;
+          }
+          if (bmh) {
+            float ee;
+            fp += born(r2, bi, bmht[j], qqf * pi.w * pj.w, &ee);
+            any = true;
+          }
+          bucket = 1;
+        } else if (iion != jion) {
+          if (vi) {
+            float ee;
+            fp = lj_coul(r2, x.c.ljA[ti * nt + tj], x.c.ljB[ti * nt + tj], qqf * pi.w * pj.w, true, &ee) * (wi * wj);
+            any = true;
+            bucket = 2;
+          }
+        } else if (mi != mj) {
+          if (vv) {
+            float ee;
+            fp = lj_coul(r2, x.c.ljA[ti * nt + tj], x.c.ljB[ti * nt + tj], qqf * pi.w * pj.w, true, &ee) * (wi * wj);
+            any = true;
+            bucket = 3;
+          }
         }
-        if (bmh) {
-          float ee;
-          fp += born(r2, bi, bmht[j], qqf * pi.w * pj.w, &ee);
-          any = true;
-        }
-        bucket = 1;
-      } else if (iion != jion) {
-        if (vi) {
-          float ee;
-          fp = lj_coul(r2, x.c.ljA[ti * nt + tj], x.c.ljB[ti * nt + tj], qqf * pi.w * pj.w, true, &ee) * (wi * wj);
-          any = true;
-          bucket = 2;
-        }
-      } else if (mi != mj) {
-        if (vv) {
-          float ee;
-          fp = lj_coul(r2, x.c.ljA[ti * nt + tj], x.c.ljB[ti * nt + tj], qqf * pi.w * pj.w, true, &ee) * (wi * wj);
-          any = true;
-          bucket = 3;
+        if (any) {
+          long long fx, fy, fz;
+          if constexpr (FP64) {
+            /* the same terms in FP64 from the FP64 positions and tables */
+            const double ex = xd[0] - x.c.x[3 * j], ey = xd[1] - x.c.x[3 * j + 1], ez = xd[2] - x.c.x[3 * j + 2];
+            const double R2d = ex * ex + ey * ey + ez * ez;
+            const double qq = P->qqrd2e * qid * charge_d(x, j);
+            const double Ad = x.db[P->d_ljA + ti * nt + tj], Bd = x.db[P->d_ljB + ti * nt + tj];
+            double fd = 0.0;
+            if (bucket == 1) {
+              if (amber && !((x.c.excl[i * P->excl_words + (j >> 5)] >> (j & 31)) & 1u))
+                fd += lj_coul_d(R2d, Ad, Bd, qq, true);
+              if (bmh) fd += born_d(R2d, bi, bmht[j], qq);
+            } else {
+              fd = lj_coul_d(R2d, Ad, Bd, qq, true) * (wid * weight_d(x, j));
+            }
+            fx = fixd(fd * ex);
+            fy = fixd(fd * ey);
+            fz = fixd(fd * ez);
+          } else {
+            fx = fixf(fp * dx);
+            fy = fixf(fp * dy);
+            fz = fixf(fp * dz);
+          }
+          F0 += fx; F1 += fy; F2 += fz;
+          R0 -= fx; R1 -= fy; R2 -= fz;
+          if (eflag) {
+            const double R2e = r2d(x.c.x + 3 * i, x.c.x + 3 * j);
+            const double qi = i < ni ? x.db[P->d_ion_q + i] : x.db[P->d_vap_q + (i - ni) % P->a_v];
+            const double qj = j < ni ? x.db[P->d_ion_q + j] : x.db[P->d_vap_q + (j - ni) % P->a_v];
+            const double qq = P->qqrd2e * qi * qj;
+            double ed = 0;
+            if (bucket == 1) {
+              if (amber && !((x.c.excl[i * P->excl_words + (j >> 5)] >> (j & 31)) & 1u))
+                ed += lj_coul_energy(R2e, x.db[P->d_ljA + ti * nt + tj], x.db[P->d_ljB + ti * nt + tj], qq);
+              if (bmh) ed += born_energy(R2e, bi, bmht[j], qq);
+              e_ion += efixd(ed);
+            } else {
+              ed = lj_coul_energy(R2e, x.db[P->d_ljA + ti * nt + tj], x.db[P->d_ljB + ti * nt + tj], qq);
+              if (bucket == 2) e_vi += efixd(ed);
+              else e_vv += efixd(ed);
+            }
+          }
         }
       }
-      if (!any) continue;
-      if constexpr (FP64) {
-        /* the same terms in FP64 from the FP64 positions and tables */
-        const double ex = xd[0] - x.c.x[3 * j], ey = xd[1] - x.c.x[3 * j + 1], ez = xd[2] - x.c.x[3 * j + 2];
-        const double R2 = ex * ex + ey * ey + ez * ez;
-        const double qq = P->qqrd2e * qid * charge_d(x, j);
-        const double Ad = x.db[P->d_ljA + ti * nt + tj], Bd = x.db[P->d_ljB + ti * nt + tj];
-        double fd = 0.0;
-        if (bucket == 1) {
-          if (amber && !((x.c.excl[i * P->excl_words + (j >> 5)] >> (j & 31)) & 1u)) fd += lj_coul_d(R2, Ad, Bd, qq, true);
-          if (bmh) fd += born_d(R2, bi, bmht[j], qq);
-        } else {
-          fd = lj_coul_d(R2, Ad, Bd, qq, true) * (wid * weight_d(x, j));
-        }
-        F0 += fixd(fd * ex);
-        F1 += fixd(fd * ey);
-        F2 += fixd(fd * ez);
-      } else {
-        F0 += fixf(fp * dx);
-        F1 += fixf(fp * dy);
-        F2 += fixf(fp * dz);
-      }
-      if (eflag && j > i) {
-        const double R2 = r2d(x.c.x + 3 * i, x.c.x + 3 * j);
-        const double qi = i < ni ? x.db[P->d_ion_q + i] : x.db[P->d_vap_q + (i - ni) % P->a_v];
-        const double qj = j < ni ? x.db[P->d_ion_q + j] : x.db[P->d_vap_q + (j - ni) % P->a_v];
-        const double qq = P->qqrd2e * qi * qj;
-        double ed = 0;
-        if (bucket == 1) {
-          if (amber && !((x.c.excl[i * P->excl_words + (j >> 5)] >> (j & 31)) & 1u))
-            ed += lj_coul_energy(R2, x.db[P->d_ljA + ti * nt + tj], x.db[P->d_ljB + ti * nt + tj], qq);
-          if (bmh) ed += born_energy(R2, bi, bmht[j], qq);
-          e_ion += efixd(ed);
-        } else {
-          ed = lj_coul_energy(R2, x.db[P->d_ljA + ti * nt + tj], x.db[P->d_ljB + ti * nt + tj], qq);
-          if (bucket == 2) e_vi += efixd(ed);
-          else e_vv += efixd(ed);
-        }
-      }
+      R0 = __shfl_sync(0xffffffffu, R0, (lane + 1) & 31);
+      R1 = __shfl_sync(0xffffffffu, R1, (lane + 1) & 31);
+      R2 = __shfl_sync(0xffffffffu, R2, (lane + 1) & 31);
     }
     if (act && (F0 | F1 | F2)) {
       const long long F[3] = {F0, F1, F2};
       acc_add(x, i, F);
+    }
+    const int jj = jb * 32 + lane;
+    if (jj < nc && (R0 | R1 | R2)) {
+      const long long Rv[3] = {R0, R1, R2};
+      acc_add(x, jj, Rv);
     }
   }
   if (eflag) {
@@ -900,8 +905,8 @@ __device__ __forceinline__ double gas_intra(const Ctx& x, const double* X, doubl
   }
 }
 
-/* SHAKE of a two-atom gas molecule, the sweeps of shake_small with one colour */
-__device__ __forceinline__ int shake_gas2(const Ctx& x, double* X, const double* R, const double* m) {
+/* SHAKE of a two-atom gas molecule: the sweeps of the vapor SHAKE with one colour */
+__device__ __forceinline__ int shake_gas2(const Ctx& x, double* X, const double* R) {
   const RepParams* P = x.P;
   const int* rigid = x.ib + P->o_gas_rigid;
   const int n = P->n_gas_rigid;
@@ -916,7 +921,7 @@ __device__ __forceinline__ int shake_gas2(const Ctx& x, double* X, const double*
         RY[q] = sw ? R[3 + q] : R[q];
         RY[3 + q] = sw ? R[q] : R[3 + q];
       }
-      shake_pair(Y, RY, 0, 1, x.db[P->d_bond + 2 * rigid[3 * k + 2] + 1], sw ? m[1] : m[0], sw ? m[0] : m[1]);
+      shake_pair_c(Y, Y + 3, RY, RY + 3, x.db + P->d_gas_cons + 3 * k);
       for (int q = 0; q < 3; q++) {
         X[q] = sw ? Y[3 + q] : Y[q];
         X[3 + q] = sw ? Y[q] : Y[3 + q];
@@ -924,7 +929,7 @@ __device__ __forceinline__ int shake_gas2(const Ctx& x, double* X, const double*
     }
     converge = true;
     for (int k = 0; k < n; k++)
-      if (shake_residual(X, 0, 1, x.db[P->d_bond + 2 * rigid[3 * k + 2] + 1]) > 1e-20) converge = false;
+      if (shake_res_c(X, X + 3, x.db + P->d_gas_cons + 3 * k) > 1e-20) converge = false;
   }
   return converge ? 0 : MDN_ST_SHAKE_NOCONV;
 }
@@ -973,7 +978,7 @@ __device__ void gas_integrate_t(Ctx& x, bool fused, bool eflag) {
         double Xd[3 * AG];
 #pragma unroll
         for (int q = 0; q < 3 * ag; q++) Xd[q] = X[q];
-        int st = shake_gas2(x, X, R, m);
+        int st = shake_gas2(x, X, R);
         if (st) set_status(x, st);
         if (vcorr)
 #pragma unroll

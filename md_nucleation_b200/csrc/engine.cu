@@ -476,6 +476,20 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
       for (int i = 0; i < n; i++) dblob.push_back(p[i]);
       return o;
     };
+    /* SHAKE constraint tables: d^2, 1/m_i, 1/m_j of each rigid pair */
+    auto cons_table = [&](const mdn_topology& t) {
+      std::vector<double> c(3 * (size_t)std::max(t.n_rigid, 1), 0.0);
+      for (int k = 0; k < t.n_rigid; k++) {
+        const double dk = d.bond_coeff[2 * t.rigid[3 * k + 2] + 1];
+        c[3 * k] = dk * dk;
+        c[3 * k + 1] = 1.0 / d.atom_mass[t.type[t.rigid[3 * k]]];
+        c[3 * k + 2] = 1.0 / d.atom_mass[t.type[t.rigid[3 * k + 1]]];
+      }
+      return dpush(c.data(), (int)c.size());
+    };
+    P.d_ion_cons = cons_table(d.ion);
+    P.d_gas_cons = cons_table(d.gas);
+    P.d_vap_cons = d.n_vapor > 0 ? cons_table(d.vapor) : P.d_ion_cons;
     P.d_bond = dpush(d.bond_coeff, 2 * d.n_bond_types);
     P.d_angle = dpush(d.angle_coeff, 2 * d.n_angle_types);
     P.d_dih = dpush(d.dihedral_coeff, 15 * d.n_dihedral_types);

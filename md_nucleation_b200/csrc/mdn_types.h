@@ -73,6 +73,7 @@ typedef struct RepParams {
   /* offsets inside the double blob */
   int d_bond, d_angle, d_dih, d_ljA, d_ljB, d_mass, d_c2;
   int d_ion_q, d_gas_x, d_gas_q, d_vap_x, d_vap_q;
+  int d_ion_cons, d_gas_cons, d_vap_cons; /* per SHAKE constraint: d^2, 1/m_i, 1/m_j */
   int pad0;
   /* run parameters */
   double dt, box, ml2, ri2, RI2, rcenter, overlap, margin;
