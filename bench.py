@@ -314,6 +314,57 @@ def plain_sample(engine, specs, quirks, n_pick: int):
     return atom_steps / seconds, sample
 
 
+PLACE_GAS, PLACE_VAPOR, PLACE_REF_GAS, PLACE_REF_VAPOR = 1_000_000, 1000, 20_000, 100
+
+
+def placement_measurement(engine):
+    """Initial placement of the configuration-4 system (1,000,000 N2 and
+    1,000 water around the 500-atom chain, 300 K, 1e5 Pa) through mdn_place,
+    host buffers in and out, against the reference's own
+    MD::initialization_gas / initialization_vapor timed on a bounded sample
+    (their loop scans every row placed so far for every candidate, so the
+    cost grows with the square of the molecule count)."""
+    import ctypes as C
+    import math
+    from md_nucleation_b200 import generate
+    from md_nucleation_b200.system import GAS_TABLE, mb_mass_kg
+    T = 300.0
+    box = generate.box_from_pressure(PLACE_GAS, T, 1e5)
+    spec = generate.config4_replica(0, n_gas=2000, n_vap=10)  # the configuration-4 ion, placed in its box
+    spec.box = box
+    ion = spec.ion.x
+    sg = math.sqrt(1.38e-23 * T / mb_mass_kg(GAS_TABLE["N2"]["mol_mass"]))
+    sv = math.sqrt(1.38e-23 * T / spec.vapor_mb_mass)
+    engine.place(box, ion, 1000, 10, sg, sv, 1)  # loads the kernels
+    times = []
+    for rep in range(3):
+        t0 = time.perf_counter()
+        engine.place(box, ion, PLACE_GAS, PLACE_VAPOR, sg, sv, 0x4D444E55 + 4000 + rep)
+        times.append(time.perf_counter() - t0)
+    t = statistics.median(times)
+    n = PLACE_GAS + PLACE_VAPOR
+    out = {"workload": f"configuration 4: {PLACE_GAS:,} N2 + {PLACE_VAPOR:,} water around a {len(ion)}-atom "
+                       f"chain, box {box:.0f} A",
+           "value": n / t, "unit": "molecules/s", "seconds": t,
+           "measured": "mdn_place wall time, host buffers in and out (device buffers allocated in the call)"}
+    from oracle import bind
+    if bind.have_reference():
+        L = bind.ref_lib()
+        L.ref_time_placement.restype = C.c_double
+        L.ref_time_placement.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        d, keep = spec.to_desc()
+        with stdout_to_stderr():
+            s = L.ref_time_placement(C.addressof(d), PLACE_REF_GAS, PLACE_REF_VAPOR)
+        m = PLACE_REF_GAS + PLACE_REF_VAPOR
+        out["reference"] = {
+            "seconds": s, "molecules": m, "value": m / s, "unit": "molecules/s", "cores": 1,
+            "sample": f"{PLACE_REF_GAS:,} N2 + {PLACE_REF_VAPOR} water in the same box around the same chain, "
+                      "MD::initialization_gas / initialization_vapor as shipped",
+            "full_size_estimate_s": s * (n / m) ** 2,
+        }
+    return out
+
+
 def adjoint_measurement(engine):
     """The gradient harness on the adjoint configuration: a 2,000-step window
     of the production system (150-atom +1 chain, 100 methanol, 100,000 rigid
@@ -462,6 +513,10 @@ def run_engine(args):
     cap = int(atoms1.max() * 1.5 * eng.n) + 1024
     snap = engine.SnapshotBuffer(eng.n, cap, pinned=True)
     e2e_steps = max(1, min(args.steps, 3))
+    # one untimed pass loads the snapshot kernels and touches the host pages
+    eng.set_nvt_batch(modes.array, temps.array)
+    eng.step(MD_STEPS, energy_mode=1)
+    eng.snapshot(snap, energies=True)
     barrier()
     t0 = time.perf_counter()
     d2h = 0
@@ -537,6 +592,9 @@ def run_engine(args):
     # the gradient harness's cost against its own forward window (rank 0, N = 1)
     if rank == 0 and ws == 1 and not args.no_adjoint:
         out["adjoint"] = adjoint_measurement(engine)
+    # initial placement of the configuration-4 system (rank 0, N = 1)
+    if rank == 0 and ws == 1 and not args.no_placement:
+        out["placement"] = placement_measurement(engine)
     # CPU baseline on rank 0 at N = 1 only
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         from oracle import bind
@@ -568,6 +626,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the one-system-per-launch measurement")
     ap.add_argument("--plain-replicas", type=int, default=16)
     ap.add_argument("--no-adjoint", action="store_true", help="skip the gradient-harness measurement")
+    ap.add_argument("--no-placement", action="store_true", help="skip the initial-placement measurement")
     ap.add_argument("--cluster", type=int, default=0, help="CTAs per replica (1..8); 0 = tuned in the warm-up")
     args = ap.parse_args()
     if args.warmup < 3 and not os.environ.get("MDN_BENCH_ALLOW_SHORT"):

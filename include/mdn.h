@@ -371,6 +371,43 @@ int  mdn_events(mdn_handle* h, mdn_event* ev, int capacity, int* count);
  * out[4*r + 0..3] = Kion, Kgas, Kvap (kcal/mol) and Tion (K).             */
 int  mdn_kinetic(mdn_handle* h, double* out);
 
+/* ---- initial placement ---------------------------------------------------- */
+/* Initial centres and velocities of the gas and vapor molecules on the GPU,
+ * replacing MD::initialization_gas / MD::initialization_vapor
+ * (src/initialization/initializationGas.cpp:24-100,
+ * src/initialization/initializationVapor.cpp:14-76).
+ *
+ * The reference draws centres uniformly in the cube and keeps one when every
+ * row of its atom table is farther than min_dist (10 A), minimum image.  The
+ * rows are the ion's atoms and, for each molecule already placed, its atoms
+ * at the origin.  So a centre is kept when it is farther than min_dist from
+ * every ion atom and, once any molecule is placed, from the origin.  Gas is
+ * placed first, then vapor.
+ *
+ * The candidates come from a counter-based stream (Philox4x32-10, Salmon et
+ * al., SC'11), so candidate k is tested independently of the others; the
+ * molecules are the first n_gas (n_vapor) kept candidates in stream order.
+ * Positions do not depend on the launch shape.  Centre velocities are
+ * Maxwell-Boltzmann: sigma * N(0,1) * 1e-5 A/fs per component, the normal
+ * deviates by Box-Muller from the same stream.
+ *
+ * ion_x, gas_x, gas_v, vapor_x, vapor_v are host arrays ([3*n]).
+ * MDN_ERR_ARG when more than 1000 * (n + 10) candidates are drawn for a
+ * species (the reference would loop for ever); MDN_ERR_NO_DEVICE without a
+ * GPU.  Allocates device memory for the call and frees it before return. */
+typedef struct mdn_place_desc {
+  double box;                   /* cube edge (A); centres in [-box/2, box/2]   */
+  double min_dist;              /* 10 A in the reference                      */
+  int n_ion;                    /* ion atoms (after the ion's rotation)       */
+  const double* ion_x;          /* [3*n_ion]                                  */
+  int n_gas, n_vapor;
+  double gas_sigma;             /* sqrt(kB T / m_gas) (m/s), m per molecule   */
+  double vapor_sigma;           /* sqrt(kB T / m_vapor) (m/s)                 */
+  unsigned long long seed;      /* keys the stream                            */
+} mdn_place_desc;
+int  mdn_place(int device, const mdn_place_desc* d, double* gas_x, double* gas_v, double* vapor_x,
+               double* vapor_v);
+
 /* ---- timing / tuning ------------------------------------------------------ */
 /* Device time (ms) of the last mdn_step, measured with CUDA events on the
  * stream the kernels were launched on; kernel_launches = kernels issued.  */

@@ -117,6 +117,14 @@ class State(C.Structure):
     ]
 
 
+class PlaceDesc(C.Structure):
+    _fields_ = [
+        ("box", C.c_double), ("min_dist", C.c_double), ("n_ion", C.c_int), ("ion_x", _dp),
+        ("n_gas", C.c_int), ("n_vapor", C.c_int), ("gas_sigma", C.c_double), ("vapor_sigma", C.c_double),
+        ("seed", C.c_ulonglong),
+    ]
+
+
 class Event(C.Structure):
     _fields_ = [
         ("replica", C.c_int), ("molecule", C.c_int), ("kind", C.c_int), ("pad", C.c_int),

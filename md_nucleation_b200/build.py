@@ -15,7 +15,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libmdn.so")
-SOURCES = ["advance.cu", "advance_fp64.cu", "snapshot.cu", "snapshot_noalloc.cu", "adjoint.cu", "engine.cu"]
+SOURCES = ["advance.cu", "advance_fp64.cu", "snapshot.cu", "snapshot_noalloc.cu", "adjoint.cu", "place.cu", "engine.cu"]
 HOST = os.path.join(HERE, "host")
 HOST_SOURCES = ["mdn_host.cpp"]
 HOST_LIB = os.path.join(LIB_DIR, "libmdn_host.so")

@@ -72,6 +72,8 @@ def lib():
         L.mdn_host_free.argtypes = [C.c_void_p]
         L.mdn_set_nvt_batch.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_double)]
         L.mdn_profile.argtypes = [vp, C.c_int, C.POINTER(C.c_longlong)]
+        dp = C.POINTER(C.c_double)
+        L.mdn_place.argtypes = [C.c_int, C.POINTER(abi.PlaceDesc), dp, dp, dp, dp]
         if L.mdn_abi_version() != abi.ABI_VERSION:
             raise RuntimeError("libmdn.so ABI version mismatch")
         _LIB = L
@@ -87,6 +89,20 @@ def device_count() -> int:
     n = C.c_int(0)
     lib().mdn_device_count(C.byref(n))
     return n.value
+
+
+def place(box, ion_x, n_gas, n_vapor, gas_sigma, vapor_sigma, seed, min_dist=10.0, device=0):
+    """Initial centres and velocities of the gas and vapor molecules on the
+    GPU (mdn_place): MD::initialization_gas / initialization_vapor
+    (src/initialization/initializationGas.cpp:24-100,
+    src/initialization/initializationVapor.cpp:14-76).  Returns
+    (gas_x, gas_v, vapor_x, vapor_v), each [n, 3] float64."""
+    ion = np.ascontiguousarray(ion_x, np.float64).reshape(-1, 3)
+    d = abi.PlaceDesc(box=box, min_dist=min_dist, n_ion=len(ion), ion_x=abi.ptr(ion), n_gas=n_gas,
+                      n_vapor=n_vapor, gas_sigma=gas_sigma, vapor_sigma=vapor_sigma, seed=seed)
+    out = [np.zeros((n, 3)) for n in (n_gas, n_gas, n_vapor, n_vapor)]
+    _ck(lib().mdn_place(device, C.byref(d), *[abi.ptr(a) for a in out]))
+    return tuple(out)
 
 
 def default_options(**kw) -> abi.Options:

@@ -40,6 +40,7 @@ def lib():
         L = C.CDLL(HOST_LIB)
         vp = C.c_void_p
         L.mdnh_load.argtypes = [C.c_char_p, C.c_int, C.c_ulonglong, C.c_int, C.POINTER(vp)]
+        L.mdnh_load_ex.argtypes = [C.c_char_p, C.c_int, C.c_ulonglong, C.c_int, C.c_int, C.POINTER(vp)]
         L.mdnh_free.argtypes = [vp]
         L.mdnh_free.restype = None
         L.mdnh_last_error.restype = C.c_char_p
@@ -75,13 +76,16 @@ def _arr(ptr, n, dtype):
 
 
 class HostSystem:
-    """One system read from a condition file (and the files it names)."""
+    """One system read from a condition file (and the files it names).
+    place_device >= 0 places the molecules on that GPU (mdn_place), -1 on
+    the CPU."""
 
-    def __init__(self, condition_file: str, calc_number: int = 0, seed: int = 0, reference_masses: bool = False):
+    def __init__(self, condition_file: str, calc_number: int = 0, seed: int = 0, reference_masses: bool = False,
+                 place_device: int = -1):
         self.L = lib()
         h = C.c_void_p()
-        _ck(self.L.mdnh_load(condition_file.encode(), calc_number, seed, 1 if reference_masses else 0,
-                             C.byref(h)))
+        _ck(self.L.mdnh_load_ex(condition_file.encode(), calc_number, seed, 1 if reference_masses else 0,
+                                place_device, C.byref(h)))
         self.h = h
 
     def close(self):

@@ -449,7 +449,7 @@ void rotation(double a, double b, double c, double* v) {
   v[2] = z2;
 }
 
-int place(mdnh_system* s, std::mt19937_64& rng) {
+int place(mdnh_system* s, std::mt19937_64& rng, int place_device) {
   const double L = s->set.box, half = 0.5 * L, dis = 10.0;
   const int ni = (int)s->ion.type.size();
   /* orientation of the ion about the origin, uniform on SO(3) */
@@ -463,9 +463,32 @@ int place(mdnh_system* s, std::mt19937_64& rng) {
       for (int k = 0; k < 3; k++) s->ion.v[3 * i + k] = n(rng) * 1e-5;
     }
   }
+  const int ng = s->set.n_gas, nv = s->set.n_vapor;
+  const double gsig = sqrt(kb * s->T / s->gas_mb_mass), vsig = sqrt(kb * s->T / s->vap_mb_mass);
+  if (place_device >= 0) {
+    mdn_place_desc d;
+    memset(&d, 0, sizeof d);
+    d.box = L;
+    d.min_dist = dis;
+    d.n_ion = ni;
+    d.ion_x = s->ion.x.data();
+    d.n_gas = ng;
+    d.n_vapor = nv;
+    d.gas_sigma = gsig;
+    d.vapor_sigma = vsig;
+    d.seed = s->seed;
+    s->gas_x.assign(3 * (size_t)ng, 0.0);
+    s->gas_v.assign(3 * (size_t)ng, 0.0);
+    s->vap_x.assign(3 * (size_t)nv, 0.0);
+    s->vap_v.assign(3 * (size_t)nv, 0.0);
+    int rc = mdn_place(place_device, &d, s->gas_x.data(), s->gas_v.data(), s->vap_x.data(), s->vap_v.data());
+    if (rc) return fail(rc, "placement on device %d: %s", place_device, mdn_last_error());
+    return MDN_OK;
+  }
   /* a centre is kept when it is farther than 10 A (minimum image) from every
-   * ion atom and from the origin, where the reference's atom table holds the
-   * not yet inserted molecules' atoms */
+   * row of the reference's atom table: the ion atoms and, once a molecule
+   * is placed, the origin, where the not yet inserted molecules' atoms sit */
+  long long placed = 0;
   auto ok = [&](const double* X) {
     auto d2 = [&](const double* a) {
       double d[3];
@@ -477,14 +500,14 @@ int place(mdnh_system* s, std::mt19937_64& rng) {
       return d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
     };
     const double o[3] = {0, 0, 0};
-    if (d2(o) <= dis * dis) return false;
+    if (placed > 0 && sqrt(d2(o)) <= dis) return false;
     for (int i = 0; i < ni; i++)
-      if (d2(&s->ion.x[3 * i]) <= dis * dis) return false;
+      if (sqrt(d2(&s->ion.x[3 * i])) <= dis) return false;
     return true;
   };
   std::uniform_real_distribution<double> r(-half, half);
-  auto fill = [&](int n, double mb_mass, std::vector<double>& xs, std::vector<double>& vs, const char* what) {
-    std::normal_distribution<double> dist(0.0, sqrt(kb * s->T / mb_mass));
+  auto fill = [&](int n, double sigma, std::vector<double>& xs, std::vector<double>& vs, const char* what) {
+    std::normal_distribution<double> dist(0.0, sigma);
     xs.clear();
     vs.clear();
     long long tries = 0;
@@ -495,12 +518,13 @@ int place(mdnh_system* s, std::mt19937_64& rng) {
       if (!ok(X)) continue;
       xs.insert(xs.end(), X, X + 3);
       for (int k = 0; k < 3; k++) vs.push_back(dist(rng) * 1e-5);
+      placed++;
     }
     return MDN_OK;
   };
-  int rc = fill(s->set.n_gas, s->gas_mb_mass, s->gas_x, s->gas_v, "gas");
+  int rc = fill(ng, gsig, s->gas_x, s->gas_v, "gas");
   if (rc) return rc;
-  return fill(s->set.n_vapor, s->vap_mb_mass, s->vap_x, s->vap_v, "vapor");
+  return fill(nv, vsig, s->vap_x, s->vap_v, "vapor");
 }
 
 void topo(mdn_topology* t, const Molecule& m) {
@@ -588,6 +612,11 @@ const char* mdnh_last_error(void) { return g_err.c_str(); }
 
 int mdnh_load(const char* condition_file, int calc_number, unsigned long long seed, int reference_masses,
               mdnh_system** out) {
+  return mdnh_load_ex(condition_file, calc_number, seed, reference_masses, -1, out);
+}
+
+int mdnh_load_ex(const char* condition_file, int calc_number, unsigned long long seed, int reference_masses,
+                 int place_device, mdnh_system** out) {
   if (!condition_file || !out) return fail(MDN_ERR_ARG, "null argument");
   *out = nullptr;
   mdnh_system* s = new mdnh_system();
@@ -619,7 +648,7 @@ int mdnh_load(const char* condition_file, int calc_number, unsigned long long se
   s->vap_com_mass = mv;
   s->vap_mb_mass = mv / Nw / 1000.0;
   std::mt19937_64 rng(s->seed);
-  rc = place(s, rng);
+  rc = place(s, rng, place_device);
   if (rc) {
     delete s;
     return rc;

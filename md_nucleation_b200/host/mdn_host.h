@@ -49,6 +49,12 @@ typedef struct mdnh_settings {
  * molecular masses (src/constants.hpp:34) instead of the atom-mass sum.     */
 int mdnh_load(const char* condition_file, int calc_number, unsigned long long seed, int reference_masses,
               mdnh_system** out);
+/* As mdnh_load, with the gas and vapor placed on GPU place_device by
+ * mdn_place (counter-based stream, include/mdn.h) when place_device >= 0;
+ * -1 places them on the CPU as mdnh_load does.  Both follow the reference's
+ * acceptance rule; the two streams differ, so the systems do too. */
+int mdnh_load_ex(const char* condition_file, int calc_number, unsigned long long seed, int reference_masses,
+                 int place_device, mdnh_system** out);
 void mdnh_free(mdnh_system* s);
 const char* mdnh_last_error(void);
 

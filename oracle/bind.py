@@ -191,6 +191,9 @@ def orc_lib():
         L.orc_objective.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_double]
         L.orc_window.restype = C.c_double
         L.orc_window.argtypes = [vp, C.c_longlong, C.c_double, C.c_double, C.c_double, C.c_double]
+        dp = C.POINTER(C.c_double)
+        L.orc_place.restype = C.c_int
+        L.orc_place.argtypes = [C.POINTER(abi.PlaceDesc), dp, dp, dp, dp]
         _orc = L
     return _orc
 
@@ -303,6 +306,18 @@ def orc_philox(key, ctr):
     out = (C.c_uint * 4)()
     orc_lib().orc_philox(key, (C.c_uint * 4)(*ctr), out)
     return list(out)
+
+
+def orc_place(box, ion_x, n_gas, n_vapor, gas_sigma, vapor_sigma, seed, min_dist=10.0):
+    """The restated placement loop (orc_place): (gas_x, gas_v, vapor_x,
+    vapor_v) as [n, 3] arrays, or RuntimeError when it does not converge."""
+    ion = np.ascontiguousarray(ion_x, np.float64).reshape(-1, 3)
+    d = abi.PlaceDesc(box=box, min_dist=min_dist, n_ion=len(ion), ion_x=abi.ptr(ion), n_gas=n_gas,
+                      n_vapor=n_vapor, gas_sigma=gas_sigma, vapor_sigma=vapor_sigma, seed=seed)
+    out = [np.zeros((n, 3)) for n in (n_gas, n_gas, n_vapor, n_vapor)]
+    if orc_lib().orc_place(C.byref(d), *[abi.ptr(a) for a in out]) != 0:
+        raise RuntimeError("placement did not converge")
+    return tuple(out)
 
 
 def orc_step_many(replicas, n_steps, threads=0):

@@ -1238,4 +1238,64 @@ void orc_philox(unsigned long long key, const unsigned* ctr, unsigned* out) {
   for (int k = 0; k < 4; k++) out[k] = r.v[k];
 }
 
+/* Initial placement, MD::initialization_gas / initialization_vapor
+ * (src/initialization/initializationGas.cpp:24-100,
+ * src/initialization/initializationVapor.cpp:14-76), one candidate at a time
+ * as the reference loops: the candidate's minimum image distance to every
+ * row of the atom table (the ion's atoms, then one row at the origin per
+ * molecule already placed) starts at 10000 and keeps the smallest; the
+ * candidate is kept when it exceeds min_dist.  The candidates and the
+ * velocities come from the stream that mdn_place (include/mdn.h) names:
+ * key (seed lo, seed hi); counter (k lo, k hi, purpose, 0x706c6163) with
+ * purpose 0 / 1 the gas / vapor centres (x, y, z = (u01(w0..w2) - 0.5) *
+ * box), 2 / 3 the gas / vapor velocities of molecule k (Box-Muller on
+ * (w0, w1) -> vx, vy and on (w2, w3) -> vz; times sigma, then 1e-5).
+ * Returns 0, or -1 when a species needs more than 1000 * (n + 10) draws. */
+int orc_place(const mdn_place_desc* p, double* gas_x, double* gas_v, double* vap_x, double* vap_v) {
+  const uint32_t k0 = (uint32_t)(p->seed & 0xffffffffull), k1 = (uint32_t)(p->seed >> 32);
+  const double L = p->box, LH = 0.5 * L;
+  long long placed_rows = 0; /* molecules in the table, all at the origin */
+  for (int sp = 0; sp < 2; sp++) {
+    const long long n = sp == 0 ? p->n_gas : p->n_vapor;
+    double* X = sp == 0 ? gas_x : vap_x;
+    double* V = sp == 0 ? gas_v : vap_v;
+    const double sigma = sp == 0 ? p->gas_sigma : p->vapor_sigma;
+    const long long cap = 1000LL * (n + 10);
+    long long i = 0, k = 0;
+    while (i < n) {
+      if (k >= cap) return -1;
+      orc::U4 c = {{(uint32_t)k, (uint32_t)((unsigned long long)k >> 32), (uint32_t)sp, 0x706c6163u}};
+      orc::U4 w = orc::philox4x32_10(c, k0, k1);
+      k++;
+      double Xc[3];
+      for (int d = 0; d < 3; d++) Xc[d] = (orc::u01(w.v[d]) - 0.5) * L;
+      double min_dis = 10000.0;
+      auto row = [&](double ax, double ay, double az) {
+        double dx = ax - Xc[0], dy = ay - Xc[1], dz = az - Xc[2];
+        if (dx < -LH) dx += L;
+        if (dx > LH) dx -= L;
+        if (dy < -LH) dy += L;
+        if (dy > LH) dy -= L;
+        if (dz < -LH) dz += L;
+        if (dz > LH) dz -= L;
+        double dd = std::sqrt(dx * dx + dy * dy + dz * dz);
+        if (dd < min_dis) min_dis = dd;
+      };
+      for (int a = 0; a < p->n_ion; a++) row(p->ion_x[3 * a], p->ion_x[3 * a + 1], p->ion_x[3 * a + 2]);
+      if (placed_rows > 0) row(0.0, 0.0, 0.0);
+      if (!(min_dis > p->min_dist)) continue;
+      for (int d = 0; d < 3; d++) X[3 * i + d] = Xc[d];
+      orc::U4 cv = {{(uint32_t)i, (uint32_t)((unsigned long long)i >> 32), (uint32_t)(2 + sp), 0x706c6163u}};
+      orc::U4 wv = orc::philox4x32_10(cv, k0, k1);
+      double z[4];
+      orc::box_muller(wv.v[0], wv.v[1], &z[0], &z[1]);
+      orc::box_muller(wv.v[2], wv.v[3], &z[2], &z[3]);
+      for (int d = 0; d < 3; d++) V[3 * i + d] = sigma * z[d] * 1e-5;
+      i++;
+      placed_rows++;
+    }
+  }
+  return 0;
+}
+
 }  // extern "C"

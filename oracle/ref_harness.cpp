@@ -27,6 +27,7 @@
 
 #include <cstdio>
 #include <cstdlib>
+#include <chrono>
 #include <typeinfo>
 
 /* ---- the two members of src/initialization/md.cpp this harness replaces ---- */
@@ -311,6 +312,28 @@ void ref_destroy(void* hp) {
   Harness* h = (Harness*)hp;
   delete h->md;
   delete h;
+}
+
+/* Seconds the reference's own placement takes: MD::initialization_gas and
+ * MD::initialization_vapor (src/initialization/initializationGas.cpp:24-100,
+ * src/initialization/initializationVapor.cpp:14-76) run as MD::MD calls them
+ * (src/initialization/md.cpp:27-29), placing n_gas and n_vapor molecules
+ * around the descriptor's ion in its box, on a replica built with none. */
+double ref_time_placement(const mdn_replica_desc* d, int n_gas, int n_vapor) {
+  mdn_replica_desc e = *d;
+  e.n_gas = 0;
+  e.n_vapor = 0;
+  Harness* h = (Harness*)ref_create(&e, 0);
+  if (!h) return -1.0;
+  MD* md = h->md;
+  md->Nof_around_gas = n_gas;
+  md->Nof_around_vapor = n_vapor;
+  const auto t0 = std::chrono::steady_clock::now();
+  md->initialization_gas();
+  md->initialization_vapor();
+  const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  ref_destroy(h);
+  return s;
 }
 
 /* out: n_gas_in, n_vapor_in, loopPair, loop_update, gi pairs, gv pairs, vv pairs, gg pairs */
