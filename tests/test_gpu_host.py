@@ -2,7 +2,7 @@
 
 The run writes the reference's files at the reference's cadence; the frames
 of its main run agree with the FP64 oracle started from the same descriptor
-(the host's placement for the same calculation number) through the same
+(the host's GPU placement for the same calculation number, as mdn_run does) through the same
 re-initialisation (re-centre, rebuild, NVE): to the dump's 6 decimals on the
 first frame and within 2e-5 A after 30 steps.
 """
@@ -92,7 +92,7 @@ def test_mdn_run_main_run_matches_oracle(host, oracle_libs, tmp_path):
     assert len(frames) == 2
     # MD::run advances vars->time by 10000 dt before the first frame (src/run.cpp:60-63)
     assert frames[0][0] == 10000 and frames[1][0] == 10000
-    s = host.HostSystem(cond, calc_number=9)   # the same placement
+    s = host.HostSystem(cond, calc_number=9, place_device=0)   # the same placement as mdn_run
     o = oracle_libs.OracleReplica.from_desc(s.desc_ptr())
     o.recenter(1)      # src/run.cpp:42-53
     o.make_pair()      # src/run.cpp:54
