@@ -52,7 +52,8 @@ struct Core {
   double* x;        /* [3*nc] positions                        */
   double* v;        /* [3*nc] velocities                       */
   double* f;        /* [3*nc] force of the last evaluation     */
-  long long* acc;   /* [2][3*nc] fixed-point partial sums      */
+  long long* acc;   /* [3*nc] fixed-point partial sums         */
+  unsigned* chunk;  /* [9*nc] the near pass's sums in 32-bit chunks */
   float4* pos;      /* [nc] (x - ion centre, charge), FP32     */
   float* w;         /* [nc] taper weight                       */
   int* type;        /* [nc] atom type                          */
@@ -72,7 +73,6 @@ struct Ctx {
   int r;            /* replica                          */
   int rank, C;      /* cluster rank and size            */
   int n_core;       /* atoms in the core                */
-  int buf;          /* which acc buffer holds this step */
   int* iscr;        /* >= 64 ints of scratch            */
   int* cand;        /* [MDN_INSERT_MAX_VAPOR + 1] entering vapor molecules, count last */
   double* trial;    /* [3*MDN_MAX_VAP_ATOMS] trial atoms */
@@ -234,9 +234,9 @@ __device__ __forceinline__ double shake_res_c(const double* Xi, const double* Xj
 __device__ void core_drift_shake(Ctx& x) {
   const RepParams* P = x.P;
   /* positions before the drift (the SHAKE reference vectors) live in the
-   * accumulation buffer this step's forces will use: it is zeroed only after
-   * SHAKE, and no CTA of the cluster reads it any more (see core_reduce) */
-  double* const xold = (double*)(x.c.acc + (size_t)x.buf * 3 * x.a->nc_cap);
+   * accumulation buffer: it is zeroed only after SHAKE, and no CTA of the
+   * cluster reads it any more (core_reduce ends with a cluster barrier) */
+  double* const xold = (double*)x.c.acc;
   const bool sh = (P->interactions & MDN_I_SHAKE) != 0;
   const bool vcorr = !(P->quirks & MDN_Q_SHAKE_NO_VCORR);
   const double dt = P->dt;
@@ -618,10 +618,27 @@ __device__ __forceinline__ double charge_d(const Ctx& x, int i) {
 /* forces of the core (ion + vapor) among themselves, and the core kick        */
 /* ------------------------------------------------------------------------- */
 __device__ __forceinline__ void acc_add(Ctx& x, int i, const long long* f3) {
-  long long* A = x.c.acc + (size_t)x.buf * 3 * x.a->nc_cap + 3 * i;
+  long long* A = x.c.acc + 3 * i;
   atomicAdd((unsigned long long*)&A[0], (unsigned long long)f3[0]);
   atomicAdd((unsigned long long*)&A[1], (unsigned long long)f3[1]);
   atomicAdd((unsigned long long*)&A[2], (unsigned long long)f3[2]);
+}
+
+/* acc_add for the gas molecules' reaction on the core: each 64-bit term
+ * u = lo16 + 2^16 mid16 + 2^32 hi32 goes into three 32-bit sums (32-bit
+ * shared-memory atomics are native, 64-bit ones are not).  The two 16-bit
+ * sums are exact for up to 65,536 terms (an atom takes at most one term per
+ * near molecule, and the near list holds at most 65,535); the high sum only
+ * matters modulo 2^32.  core_reduce folds them into acc exactly. */
+__device__ __forceinline__ void acc_add_chunks(Ctx& x, int i, const long long* f3) {
+  unsigned* A = x.c.chunk + 9 * i;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const unsigned long long u = (unsigned long long)f3[k];
+    atomicAdd(&A[3 * k], (unsigned)(u & 0xFFFFull));
+    atomicAdd(&A[3 * k + 1], (unsigned)((u >> 16) & 0xFFFFull));
+    atomicAdd(&A[3 * k + 2], (unsigned)(u >> 32));
+  }
 }
 
 __device__ __forceinline__ void energy_add(Ctx& x, int bucket, long long e) {
@@ -1066,7 +1083,8 @@ __device__ void gas_far_pass(Ctx& x, bool eflag, bool kick) {
  * each, walking the molecule's lists (about one entry per molecule in the
  * batched workload, so a wider split leaves lanes idle); the molecule's own
  * force stays in registers, the reaction goes to the core sums by shared
- * 64-bit integer atomics, so the result does not depend on the order */
+ * 32-bit integer atomics on exact chunks (acc_add_chunks), so the result
+ * does not depend on the order */
 template <int AG, bool FP64>
 __device__ void gas_near_pass_t(Ctx& x, bool eflag, bool kick) {
   const RepParams* P = x.P;
@@ -1142,7 +1160,7 @@ __device__ void gas_near_pass_t(Ctx& x, bool eflag, bool kick) {
             egi += efixd(lj_coul_energy(r2d(X + 3 * at, x.c.x + 3 * j), x.db[P->d_ljA + gtype[at] * nt + tj],
                                         x.db[P->d_ljB + gtype[at] * nt + tj], 0.0));
         }
-        acc_add(x, j, R);
+        acc_add_chunks(x, j, R);
       }
     }
     if (gv) {
@@ -1175,7 +1193,7 @@ __device__ void gas_near_pass_t(Ctx& x, bool eflag, bool kick) {
               egv += efixd(lj_coul_energy(r2d(X + 3 * at, x.c.x + 3 * j), x.db[P->d_ljA + gtype[at] * nt + tj],
                                           x.db[P->d_ljB + gtype[at] * nt + tj], 0.0));
           }
-          acc_add(x, j, R);
+          acc_add_chunks(x, j, R);
         }
       }
     }
@@ -1218,7 +1236,16 @@ __device__ void gas_near_pass(Ctx& x, bool eflag, bool kick) {
 /* sum of the core partials over the cluster -> f (double), identical in every CTA */
 __device__ void core_reduce(Ctx& x, cg::cluster_group& cl) {
   const int n3 = 3 * x.n_core;
-  long long* mine = x.c.acc + (size_t)x.buf * 3 * x.a->nc_cap;
+  long long* mine = x.c.acc;
+  /* fold the near pass's chunk sums into this CTA's 64-bit sums (each
+   * thread its own elements) and clear them for the next evaluation */
+  for (int q = threadIdx.x; q < n3; q += blockDim.x) {
+    unsigned* c = x.c.chunk + 3 * q;
+    const unsigned long long s =
+        (unsigned long long)c[0] + ((unsigned long long)c[1] << 16) + ((unsigned long long)c[2] << 32);
+    c[0] = c[1] = c[2] = 0;
+    mine[q] += (long long)s;
+  }
   if (x.C > 1) {
     cl.sync();
     for (int q = threadIdx.x; q < n3; q += blockDim.x) {
@@ -1229,6 +1256,9 @@ __device__ void core_reduce(Ctx& x, cg::cluster_group& cl) {
       }
       x.c.f[q] = (double)s * MDN_FIX_INV;
     }
+    /* every CTA has read this one's sums: the buffer is free again (the
+     * next step's SHAKE keeps its reference positions there) */
+    cl.sync();
   } else {
     for (int q = threadIdx.x; q < n3; q += blockDim.x) x.c.f[q] = (double)mine[q] * MDN_FIX_INV;
   }
@@ -1239,11 +1269,10 @@ __device__ void core_reduce(Ctx& x, cg::cluster_group& cl) {
       if (!(fabs(x.c.f[q]) < MDN_FIX_LIMIT)) set_status(x, MDN_ST_FIXED_OVERFLOW);
       if (!isfinite(x.c.x[q]) || !isfinite(x.c.v[q])) set_status(x, MDN_ST_NONFINITE);
     }
-  x.buf ^= 1;  /* the next evaluation accumulates into the other buffer */
 }
 
 __device__ void zero_acc(Ctx& x) {
-  long long* mine = x.c.acc + (size_t)x.buf * 3 * x.a->nc_cap;
+  long long* mine = x.c.acc;
   for (int q = threadIdx.x; q < 3 * x.n_core; q += blockDim.x) mine[q] = 0;
   __syncthreads();
 }
@@ -1958,7 +1987,8 @@ extern "C" __global__ void __launch_bounds__(512, 1) MDN_ADVANCE_KERNEL(KArgs a)
     unsigned char* p = dsm;
     const int nc = a.nc_cap;
     auto take = [&](size_t bytes) { unsigned char* q = p; p += (bytes + 15) & ~(size_t)15; return q; };
-    x.c.acc = (long long*)take(sizeof(long long) * 6 * nc);
+    x.c.acc = (long long*)take(sizeof(long long) * 3 * nc);
+    x.c.chunk = (unsigned*)take(sizeof(unsigned) * 9 * nc);
     x.c.x = (double*)take(sizeof(double) * 3 * nc);
     x.c.v = (double*)take(sizeof(double) * 3 * nc);
     x.c.f = (double*)take(sizeof(double) * 3 * nc);
@@ -1971,7 +2001,9 @@ extern "C" __global__ void __launch_bounds__(512, 1) MDN_ADVANCE_KERNEL(KArgs a)
     x.c.ljB = (float*)take(sizeof(float) * a.nt_cap * a.nt_cap);
     x.c.c2 = (double*)take(sizeof(double) * a.nt_cap);
   }
-  x.buf = 0;
+  /* the chunk sums start at zero and every core_reduce leaves them so */
+  for (int q = threadIdx.x; q < 9 * a.nc_cap; q += blockDim.x) x.c.chunk[q] = 0;
+  __syncthreads();
   for (;;) {
     if (x.rank == 0 && threadIdx.x == 0) s_job = atomicAdd(a.job_counter, 1);
     cl.sync();

@@ -172,7 +172,8 @@ size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
 /* dynamic shared memory of the kernel, carved in this order in advance.cu */
 size_t smem_bytes(int nc, int nt, int excl) {
   size_t s = 0;
-  s += align16(sizeof(long long) * 6 * nc);
+  s += align16(sizeof(long long) * 3 * nc);
+  s += align16(sizeof(unsigned) * 9 * nc);
   s += 3 * align16(sizeof(double) * 3 * nc);
   s += align16(sizeof(float4) * nc);
   s += 3 * align16(sizeof(int) * nc);
@@ -534,13 +535,15 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
     P.slab_cap = (int)std::min<double>(d.n_gas, ceil(eg * f + 6 * sqrt(eg) + 64));
     P.slab_cap = std::max(P.slab_cap, 1);
     /* in-domain vapor: binomial mean + 4 sigma (the core lives in shared memory,
-     * 148 B per atom, so this capacity is kept tight; exceeding it raises
+     * 160 B per atom, so this capacity is kept tight; exceeding it raises
      * MDN_ST_CORE_OVERFLOW) */
     double ev = d.n_vapor * frac;
     P.vcap = (int)std::min<double>(d.n_vapor, ceil(ev * (f > 1.0 ? 1.0 + 0.2 * (f - 1.0) : 1.0) +
                                                    4 * sqrt(ev * (1 - frac)) + 8));
     P.vcap = std::max(P.vcap, 1);
-    P.near_cap = P.slab_cap;
+    /* the near pass's 16-bit chunk sums are exact for up to 65,536 terms
+     * per atom, one per near molecule at most */
+    P.near_cap = std::min(P.slab_cap, 65535);
     double rion = 0;
     {
       double c[3] = {0, 0, 0};
