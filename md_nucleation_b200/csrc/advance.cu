@@ -52,8 +52,8 @@ struct Core {
   double* x;        /* [3*nc] positions                        */
   double* v;        /* [3*nc] velocities                       */
   double* f;        /* [3*nc] force of the last evaluation     */
-  long long* acc;   /* [3*nc] fixed-point partial sums         */
-  unsigned* chunk;  /* [9*nc] the near pass's sums in 32-bit chunks */
+  long long* acc;   /* [3*nc] this CTA's fixed-point force sums */
+  unsigned* chunk;  /* [9*nc] the same sums in 32-bit chunks (acc_add) */
   float4* pos;      /* [nc] (x - ion centre, charge), FP32     */
   float* w;         /* [nc] taper weight                       */
   int* type;        /* [nc] atom type                          */
@@ -234,8 +234,9 @@ __device__ __forceinline__ double shake_res_c(const double* Xi, const double* Xj
 __device__ void core_drift_shake(Ctx& x) {
   const RepParams* P = x.P;
   /* positions before the drift (the SHAKE reference vectors) live in the
-   * accumulation buffer: it is zeroed only after SHAKE, and no CTA of the
-   * cluster reads it any more (core_reduce ends with a cluster barrier) */
+   * 64-bit sum buffer: core_reduce overwrites it only after this step's
+   * forces, and no CTA of the cluster reads it any more (core_reduce ends
+   * with a cluster barrier) */
   double* const xold = (double*)x.c.acc;
   const bool sh = (P->interactions & MDN_I_SHAKE) != 0;
   const bool vcorr = !(P->quirks & MDN_Q_SHAKE_NO_VCORR);
@@ -617,20 +618,15 @@ __device__ __forceinline__ double charge_d(const Ctx& x, int i) {
 /* ------------------------------------------------------------------------- */
 /* forces of the core (ion + vapor) among themselves, and the core kick        */
 /* ------------------------------------------------------------------------- */
-__device__ __forceinline__ void acc_add(Ctx& x, int i, const long long* f3) {
-  long long* A = x.c.acc + 3 * i;
-  atomicAdd((unsigned long long*)&A[0], (unsigned long long)f3[0]);
-  atomicAdd((unsigned long long*)&A[1], (unsigned long long)f3[1]);
-  atomicAdd((unsigned long long*)&A[2], (unsigned long long)f3[2]);
-}
-
-/* acc_add for the gas molecules' reaction on the core: each 64-bit term
+/* One term of the core force sums.  Each 64-bit fixed-point term
  * u = lo16 + 2^16 mid16 + 2^32 hi32 goes into three 32-bit sums (32-bit
  * shared-memory atomics are native, 64-bit ones are not).  The two 16-bit
- * sums are exact for up to 65,536 terms (an atom takes at most one term per
- * near molecule, and the near list holds at most 65,535); the high sum only
- * matters modulo 2^32.  core_reduce folds them into acc exactly. */
-__device__ __forceinline__ void acc_add_chunks(Ctx& x, int i, const long long* f3) {
+ * sums are exact for up to 65,536 terms per atom and evaluation (one per
+ * near gas molecule, whose list holds at most 64,511, plus at most one per
+ * pair tile and per bonded term); the high sum only matters modulo 2^32.
+ * core_reduce folds the three into the 64-bit sum exactly, so the result
+ * does not depend on the order of the adds. */
+__device__ __forceinline__ void acc_add(Ctx& x, int i, const long long* f3) {
   unsigned* A = x.c.chunk + 9 * i;
 #pragma unroll
   for (int k = 0; k < 3; k++) {
@@ -1083,8 +1079,8 @@ __device__ void gas_far_pass(Ctx& x, bool eflag, bool kick) {
  * each, walking the molecule's lists (about one entry per molecule in the
  * batched workload, so a wider split leaves lanes idle); the molecule's own
  * force stays in registers, the reaction goes to the core sums by shared
- * 32-bit integer atomics on exact chunks (acc_add_chunks), so the result
- * does not depend on the order */
+ * 32-bit integer atomics on exact chunks (acc_add), so the result does not
+ * depend on the order */
 template <int AG, bool FP64>
 __device__ void gas_near_pass_t(Ctx& x, bool eflag, bool kick) {
   const RepParams* P = x.P;
@@ -1160,7 +1156,7 @@ __device__ void gas_near_pass_t(Ctx& x, bool eflag, bool kick) {
             egi += efixd(lj_coul_energy(r2d(X + 3 * at, x.c.x + 3 * j), x.db[P->d_ljA + gtype[at] * nt + tj],
                                         x.db[P->d_ljB + gtype[at] * nt + tj], 0.0));
         }
-        acc_add_chunks(x, j, R);
+        acc_add(x, j, R);
       }
     }
     if (gv) {
@@ -1193,7 +1189,7 @@ __device__ void gas_near_pass_t(Ctx& x, bool eflag, bool kick) {
               egv += efixd(lj_coul_energy(r2d(X + 3 * at, x.c.x + 3 * j), x.db[P->d_ljA + gtype[at] * nt + tj],
                                           x.db[P->d_ljB + gtype[at] * nt + tj], 0.0));
           }
-          acc_add_chunks(x, j, R);
+          acc_add(x, j, R);
         }
       }
     }
@@ -1237,14 +1233,14 @@ __device__ void gas_near_pass(Ctx& x, bool eflag, bool kick) {
 __device__ void core_reduce(Ctx& x, cg::cluster_group& cl) {
   const int n3 = 3 * x.n_core;
   long long* mine = x.c.acc;
-  /* fold the near pass's chunk sums into this CTA's 64-bit sums (each
-   * thread its own elements) and clear them for the next evaluation */
+  /* fold the chunk sums into this CTA's 64-bit sums (each thread its own
+   * elements) and clear them for the next evaluation */
   for (int q = threadIdx.x; q < n3; q += blockDim.x) {
     unsigned* c = x.c.chunk + 3 * q;
     const unsigned long long s =
         (unsigned long long)c[0] + ((unsigned long long)c[1] << 16) + ((unsigned long long)c[2] << 32);
     c[0] = c[1] = c[2] = 0;
-    mine[q] += (long long)s;
+    mine[q] = (long long)s;
   }
   if (x.C > 1) {
     cl.sync();
@@ -1271,15 +1267,8 @@ __device__ void core_reduce(Ctx& x, cg::cluster_group& cl) {
     }
 }
 
-__device__ void zero_acc(Ctx& x) {
-  long long* mine = x.c.acc;
-  for (int q = threadIdx.x; q < 3 * x.n_core; q += blockDim.x) mine[q] = 0;
-  __syncthreads();
-}
-
 /* all forces of the step (after positions and lists are final) and the second kick */
 __device__ void forces_and_kick(Ctx& x, cg::cluster_group& cl, bool eflag, bool kick) {
-  zero_acc(x);
   prof_start(x);
   gas_near_pass(x, eflag, kick);
   __syncthreads();

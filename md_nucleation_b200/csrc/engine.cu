@@ -541,9 +541,9 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
     P.vcap = (int)std::min<double>(d.n_vapor, ceil(ev * (f > 1.0 ? 1.0 + 0.2 * (f - 1.0) : 1.0) +
                                                    4 * sqrt(ev * (1 - frac)) + 8));
     P.vcap = std::max(P.vcap, 1);
-    /* the near pass's 16-bit chunk sums are exact for up to 65,536 terms
-     * per atom, one per near molecule at most */
-    P.near_cap = std::min(P.slab_cap, 65535);
+    /* the core's 16-bit chunk sums are exact for up to 65,536 terms per
+     * atom: one per near molecule at most, plus pair tiles and bonded terms */
+    P.near_cap = std::min(P.slab_cap, 64511);
     double rion = 0;
     {
       double c[3] = {0, 0, 0};
