@@ -426,7 +426,10 @@ int  mdn_tune_launch(mdn_handle* h, long long n_steps, int* best);
 /* Per-replica SM-cycle accounting of the step kernel: enable = 1 starts
  * accumulating (from zero), 0 stops.  out: [8*n_replicas] cycles per phase:
  * total, core integration, gas integration, rebuild, near gas molecules,
- * core bonded terms, core pair terms, core force sums and kick. */
+ * core bonded terms, core pair terms, core force sums and kick.  The gas
+ * molecules are integrated beside the core's constraints, so their time is
+ * counted under core integration; the gas slot holds the step's list
+ * bookkeeping only. */
 int  mdn_profile(mdn_handle* h, int enable, long long* out);
 
 #ifdef __cplusplus

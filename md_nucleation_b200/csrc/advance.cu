@@ -231,7 +231,17 @@ __device__ __forceinline__ double shake_res_c(const double* Xi, const double* Xj
   return dr * dr;
 }
 
-__device__ void core_drift_shake(Ctx& x) {
+template <int AG>
+__device__ void gas_integrate_t(Ctx& x, bool fused, bool eflag, int tid, int nthr);
+
+__device__ void gas_integrate(Ctx& x, bool fused, bool eflag, int tid, int nthr);
+
+/* Drift of the core, its constraints, and the gas integration of the step.
+ * The constraints and the gas are independent (the gas pass touches only
+ * the gas slab), so they run side by side: warp 0 sweeps the ion's
+ * constraints, the next warps take one vapor molecule per thread, and the
+ * remaining warps integrate the gas molecules. */
+__device__ void core_drift_shake(Ctx& x, bool fused, bool eflag) {
   const RepParams* P = x.P;
   /* positions before the drift (the SHAKE reference vectors) live in the
    * 64-bit sum buffer: core_reduce overwrites it only after this step's
@@ -249,53 +259,54 @@ __device__ void core_drift_shake(Ctx& x) {
     }
   }
   __syncthreads();
-  if (!sh) return;
-  /* ion: block-parallel sweeps, one colour at a time; a colour's constraints
-   * share no atom, so the sweep equals the sequential colour-ordered sweep */
-  if (P->n_ion_rigid > 0) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const bool ion_sh = sh && P->n_ion_rigid > 0;
+  const int nv = (sh && P->n_vap_rigid > 0) ? x.D->n_vap_in : 0;
+  /* warps of the ion constraints, of the vapor molecules, then of the gas */
+  const int w_ion = ion_sh ? 1 : 0;
+  const int w_vap = nv > 0 ? min((nv + 31) >> 5, max(1, (nwarps - w_ion) / 2)) : 0;
+  const int w_gas0 = min(w_ion + w_vap, nwarps - 1);
+  if (ion_sh && warp == 0) {
+    /* sweeps in colour order (a colour's constraints share no atom, so
+     * the lanes may take them in any order) until every constraint holds
+     * after a sweep */
     const int* rig = x.ib + P->o_ion_rigid;
     const int* col = x.ib + P->o_ion_color;
     int sweeps = 0;
     for (;;) {
       for (int c = 0; c < P->n_ion_colors; c++) {
-        for (int k = threadIdx.x; k < P->n_ion_rigid; k += blockDim.x) {
+        for (int k = lane; k < P->n_ion_rigid; k += 32) {
           if (col[k] != c) continue;
           int i = rig[3 * k], j = rig[3 * k + 1];
           shake_pair_c(x.c.x + 3 * i, x.c.x + 3 * j, xold + 3 * i, xold + 3 * j, x.db + P->d_ion_cons + 3 * k);
         }
-        __syncthreads();
+        __syncwarp();
       }
-      if (threadIdx.x == 0) x.iscr[50] = 1;
-      __syncthreads();
-      for (int k = threadIdx.x; k < P->n_ion_rigid; k += blockDim.x)
+      bool ok = true;
+      for (int k = lane; k < P->n_ion_rigid; k += 32)
         if (shake_res_c(x.c.x + 3 * rig[3 * k], x.c.x + 3 * rig[3 * k + 1], x.db + P->d_ion_cons + 3 * k) > 1e-20)
-          x.iscr[50] = 0;
-      __syncthreads();
-      int conv = x.iscr[50];
-      __syncthreads();
-      if (conv) break;
+          ok = false;
+      if (__all_sync(0xffffffffu, ok)) break;
       if (++sweeps >= MDN_SHAKE_MAX_SWEEPS) {
-        if (threadIdx.x == 0 && x.rank == 0) set_status(x, MDN_ST_SHAKE_NOCONV);
+        if (lane == 0 && x.rank == 0) set_status(x, MDN_ST_SHAKE_NOCONV);
         break;
       }
     }
     if (vcorr)
-      for (int i = threadIdx.x; i < P->n_ion; i += blockDim.x)
+      for (int i = lane; i < P->n_ion; i += 32)
         for (int k = 0; k < 3; k++) {
           /* displacement by the constraints = x - (xold + v*dt) */
           double xd = xold[3 * i + k] + x.c.v[3 * i + k] * dt;
           x.c.v[3 * i + k] += (x.c.x[3 * i + k] - xd) / dt;
         }
-    __syncthreads();
-  }
-  /* vapor molecules: one thread each, in place in shared memory, sweeps in
-   * colour order until every constraint holds after a sweep */
-  if (P->n_vap_rigid > 0) {
+  } else if (nv > 0 && warp >= w_ion && warp < w_ion + w_vap) {
+    /* vapor molecules: one thread each, in place in shared memory, sweeps
+     * in colour order until every constraint holds after a sweep */
     const int av = P->a_v, nr = P->n_vap_rigid, nco = P->n_vap_colors;
     const int* rig = x.ib + P->o_vap_rigid;
     const int* col = x.ib + P->o_vap_color;
     const double* ct = x.db + P->d_vap_cons;
-    for (int s = threadIdx.x; s < x.D->n_vap_in; s += blockDim.x) {
+    for (int s = threadIdx.x - 32 * w_ion; s < nv; s += 32 * w_vap) {
       const int base = P->n_ion + s * av;
       double* X = x.c.x + 3 * base;
       const double* R = xold + 3 * base;
@@ -319,6 +330,8 @@ __device__ void core_drift_shake(Ctx& x) {
           x.c.v[3 * base + q] += (X[q] - xd) / dt;
         }
     }
+  } else if (warp >= w_gas0) {
+    gas_integrate(x, fused, eflag, threadIdx.x - 32 * w_gas0, blockDim.x - 32 * w_gas0);
   }
   __syncthreads();
 }
@@ -949,8 +962,11 @@ __device__ __forceinline__ int shake_gas2(const Ctx& x, double* X, const double*
 
 /* kick + drift (+SHAKE) of the gas molecules of this CTA; far molecules also
  * get their intramolecular force and the second kick when `fused`. */
+/* kick, drift, gas SHAKE and (fused, for molecules without list entries)
+ * the intramolecular force and second kick of the gas molecules; thread tid
+ * of the nthr (whole warps) that take part */
 template <int AG>
-__device__ void gas_integrate_t(Ctx& x, bool fused, bool eflag) {
+__device__ void gas_integrate_t(Ctx& x, bool fused, bool eflag, int tid, int nthr) {
   const RepParams* P = x.P;
   const KArgs* a = x.a;
   constexpr int ag = AG;
@@ -969,7 +985,7 @@ __device__ void gas_integrate_t(Ctx& x, bool fused, bool eflag) {
     c2[at] = x.c.c2[t];
   }
   long long eg = 0;
-  for (int s = lo + threadIdx.x; s < hi; s += blockDim.x) {
+  for (int s = lo + tid; s < hi; s += nthr) {
     double X[3 * AG], V[3 * AG], F[3 * AG], R[3 * AG];
     for (int at = 0; at < ag; at++) {
       size_t g = gatom(P, par, s, at);
@@ -1023,9 +1039,9 @@ __device__ void gas_integrate_t(Ctx& x, bool fused, bool eflag) {
   }
 }
 
-__device__ void gas_integrate(Ctx& x, bool fused, bool eflag) {
-  if (x.P->a_g == 1) gas_integrate_t<1>(x, fused, eflag);
-  else gas_integrate_t<2>(x, fused, eflag);
+__device__ void gas_integrate(Ctx& x, bool fused, bool eflag, int tid, int nthr) {
+  if (x.P->a_g == 1) gas_integrate_t<1>(x, fused, eflag, tid, nthr);
+  else gas_integrate_t<2>(x, fused, eflag, tid, nthr);
 }
 
 /* after a rebuild: intramolecular force and second kick of the far molecules */
@@ -1905,7 +1921,8 @@ __device__ void one_step(Ctx& x, cg::cluster_group& cl, bool eflag) {
       for (int k = 0; k < 3; k++) x.c.v[3 * i + k] *= ratio;
     __syncthreads();
   }
-  core_drift_shake(x);
+  const bool rebuild = x.D->loop_pair + 1 > x.D->loop_update;
+  core_drift_shake(x, !rebuild, eflag);
   ion_centre(x);
   if (x.D->nvt_mode == MDN_NVT_NH) {
     double T = ion_temperature(x);
@@ -1918,10 +1935,6 @@ __device__ void one_step(Ctx& x, cg::cluster_group& cl, bool eflag) {
   core_weights_pos(x, true);
   prof_end(x, MDN_PROF_CORE_INT);
   prof_start(x);
-  const bool rebuild = x.D->loop_pair + 1 > x.D->loop_update;
-  gas_integrate(x, !rebuild, eflag);
-  __threadfence_block();
-  __syncthreads();
   if (threadIdx.x == 0) x.D->loop_pair += 1;
   __syncthreads();
   prof_end(x, MDN_PROF_GAS_INT);
