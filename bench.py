@@ -461,11 +461,13 @@ def run_engine(args):
             dist.barrier()
         torch.cuda.synchronize(device)
 
-    # warm-up: the launch-shape tuner (4 blocks of MD_STEPS, one per cluster
-    # size; results do not depend on the shape), then the warm-up steps
+    # warm-up: the launch-shape tuner (a block of MD_STEPS per cluster size,
+    # then up to 3 blocks of split launches; results do not depend on the
+    # shape), then the warm-up steps
     if args.cluster:
         eng.set_launch(args.cluster)
-        chosen_by = "--cluster"
+        eng.set_split(args.split, 2 * args.cluster if args.split else 0)
+        chosen_by = "--cluster / --split"
     else:
         tuned = eng.tune_launch(MD_STEPS)
         chosen_by = "mdn_tune_launch during warm-up"
@@ -534,6 +536,7 @@ def run_engine(args):
     e2e_value = e2e_all / e2e_s
     h2d_per_step = eng.n * (4 + 8)
     launch_shape = eng.get_launch()
+    split = eng.get_split()
 
     out = None
     if rank == 0:
@@ -552,6 +555,7 @@ def run_engine(args):
                 "parallelism": f"replicas sharded over {ws} GPU(s), no collective in the step",
                 "launch": {"cluster_ctas_per_replica": launch_shape[0], "threads_per_cta": launch_shape[1],
                            "md_steps_per_launch": MD_STEPS if launch_shape[2] <= 0 else launch_shape[2],
+                           "split": {"largest_replicas": split[0], "cluster_ctas": split[1]},
                            "chosen_by": chosen_by},
             },
             "roofline": {
@@ -628,6 +632,8 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the gradient-harness measurement")
     ap.add_argument("--no-placement", action="store_true", help="skip the initial-placement measurement")
     ap.add_argument("--cluster", type=int, default=0, help="CTAs per replica (1..8); 0 = tuned in the warm-up")
+    ap.add_argument("--split", type=int, default=0,
+                    help="with --cluster: the N largest replicas on clusters twice as large, in a concurrent launch")
     args = ap.parse_args()
     if args.warmup < 3 and not os.environ.get("MDN_BENCH_ALLOW_SHORT"):
         raise SystemExit("bench.py: --warmup must be >= 3")

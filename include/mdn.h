@@ -417,12 +417,23 @@ int  mdn_set_launch(mdn_handle* h, int cluster_size, int threads, int steps_per_
  * mdn_options.cluster_size is 0), threads per CTA, steps per launch. */
 int  mdn_get_launch(mdn_handle* h, int* cluster_size, int* threads, int* steps_per_launch);
 /* Launch-shape tuner: advances every replica by n_steps at each cluster size
- * 1, 2, 4 and 8 (4 * n_steps steps in all), timing each block with CUDA
- * events, and keeps the fastest size for later mdn_step calls; *best (may be
- * NULL) receives it.  The steps are ordinary steps of the run: results do not
- * depend on the launch shape.  A replica that fails during tuning is reported
- * as mdn_step reports it.                                                   */
+ * 1, 2, 4 and 8, timing each block with CUDA events, and keeps the fastest
+ * size for later mdn_step calls (then tries the split launch below: up to 3
+ * more blocks); *best (may be NULL) receives the cluster size.  The steps
+ * are ordinary steps of the run: results do not depend on the launch shape.
+ * A replica that fails during tuning is reported as mdn_step reports it.  */
 int  mdn_tune_launch(mdn_handle* h, long long n_steps, int* best);
+/* Split step launch: the n_largest replicas with the most estimated work
+ * run in a second launch, concurrent with the first on its own stream, on
+ * clusters of cluster_size CTAs (one cluster each), and the other replicas
+ * on the SMs left at the ordinary cluster size.  The launch of a batch is
+ * as long as its largest replica on its cluster, so giving the few largest
+ * more SMs shortens it.  n_largest = 0 turns it off.  mdn_tune_launch, when
+ * no split is set, also times n_largest = 2, 4, 8 at twice the best cluster
+ * size (n_steps each) and keeps a split that beats the best single launch.
+ * Results do not depend on the split.                                      */
+int  mdn_set_split(mdn_handle* h, int n_largest, int cluster_size);
+int  mdn_get_split(mdn_handle* h, int* n_largest, int* cluster_size);
 /* Per-replica SM-cycle accounting of the step kernel: enable = 1 starts
  * accumulating (from zero), 0 stops.  out: [8*n_replicas] cycles per phase:
  * total, core integration, gas integration, rebuild, near gas molecules,

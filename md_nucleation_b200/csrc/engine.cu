@@ -130,6 +130,13 @@ struct mdn_handle {
   int auto_cluster = 1;  /* cluster size when mdn_options.cluster_size is 0 */
   int* job_order = nullptr;
   int* job_counter = nullptr;
+  /* split step launch: the split_n largest replicas in a second, concurrent
+   * launch with clusters of split_cluster CTAs (0: one launch) */
+  int split_n = 0, split_cluster = 0;
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  int* job_order2 = nullptr;
+  int* job_counter2 = nullptr;
   std::vector<int> order;
   std::vector<int> h_iblob;
   std::vector<int> ctl_mode;
@@ -159,11 +166,14 @@ void free_all(mdn_handle* h) {
                   h->vslab_f, h->vslab_w, h->vslab_mol, h->near_list, h->near_gi, h->near_gv, h->gil_n,
                   h->gvl_n, h->gil, h->gvl, h->energy, h->events, h->n_events, h->status, h->job_order,
                   h->job_counter, h->snap_off, h->snap_type, h->snap_x, h->snap_v, h->d_ctl_mode,
-                  h->d_ctl_T, h->d_prof};
+                  h->d_ctl_T, h->d_prof, h->job_order2, h->job_counter2};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
+  if (h->stream2) cudaStreamDestroy(h->stream2);
   if (h->stream) cudaStreamDestroy(h->stream);
 }
 
@@ -205,17 +215,39 @@ int check_topology(const mdn_topology& t, int n_types, int nb, int na, int nd, c
   return MDN_OK;
 }
 
+/* one launch of the step kernel over jobs[0..n_jobs) with clusters of C
+ * CTAs on `stream`, using the given device job list and counter */
+cudaError_t launch_one(mdn_handle* h, KArgs a, const int* jobs, int n_jobs, int C, int max_clusters,
+                       int* d_order, int* d_counter, cudaStream_t stream) {
+  cudaError_t e;
+  if ((e = cudaMemcpyAsync(d_order, jobs, sizeof(int) * n_jobs, cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
+      (e = cudaMemsetAsync(d_counter, 0, sizeof(int), stream)) != cudaSuccess)
+    return e;
+  a.job_order = d_order;
+  a.n_jobs = n_jobs;
+  a.job_counter = d_counter;
+  const int clusters = std::max(1, std::min(max_clusters, n_jobs));
+  cudaLaunchConfig_t cfg;
+  memset(&cfg, 0, sizeof cfg);
+  cfg.gridDim = dim3(clusters * C);
+  cfg.blockDim = dim3(h->opt.threads);
+  cfg.dynamicSmemBytes = h->smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, h->opt.force_mode ? mdn_advance_fp64 : mdn_advance, a);
+}
+
 long long launch(mdn_handle* h, int mode, long long n_steps, int energy_mode, unsigned term_mask,
                  const std::vector<int>* jobs, int* rc, int keep_com = 0) {
   *rc = MDN_OK;
   const std::vector<int>& J = jobs ? *jobs : h->order;
   cudaError_t e;
-  if ((e = cudaMemcpyAsync(h->job_order, J.data(), sizeof(int) * J.size(), cudaMemcpyHostToDevice, h->stream)) !=
-          cudaSuccess ||
-      (e = cudaMemsetAsync(h->job_counter, 0, sizeof(int), h->stream)) != cudaSuccess) {
-    *rc = fail(MDN_ERR_CUDA, "launch setup: %s", cudaGetErrorString(e));
-    return 0;
-  }
   KArgs a;
   memset(&a, 0, sizeof a);
   a.P = h->dP;
@@ -235,9 +267,6 @@ long long launch(mdn_handle* h, int mode, long long n_steps, int energy_mode, un
   a.status = h->status;
   a.ctl_mode = h->d_ctl_mode;
   a.ctl_T = h->d_ctl_T;
-  a.job_order = h->job_order;
-  a.n_jobs = (int)J.size();
-  a.job_counter = h->job_counter;
   a.n_steps = n_steps;
   a.energy_mode = energy_mode;
   a.mode = mode;
@@ -248,23 +277,26 @@ long long launch(mdn_handle* h, int mode, long long n_steps, int energy_mode, un
   a.nt_cap = h->nt_cap;
   a.excl_cap = h->excl_cap;
   const int C = std::max(1, std::min(8, h->opt.cluster_size > 0 ? h->opt.cluster_size : h->auto_cluster));
-  int clusters = std::max(1, h->num_sms / C);
-  clusters = std::min(clusters, (int)J.size());
-  cudaLaunchConfig_t cfg;
-  memset(&cfg, 0, sizeof cfg);
-  cfg.gridDim = dim3(clusters * C);
-  cfg.blockDim = dim3(h->opt.threads);
-  cfg.dynamicSmemBytes = h->smem;
-  cfg.stream = h->stream;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = C;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  e = cudaLaunchKernelEx(&cfg, h->opt.force_mode ? mdn_advance_fp64 : mdn_advance, a);
-  if (e != cudaSuccess) {
+  const int n = (int)J.size();
+  const int nb = h->split_n, Cb = h->split_cluster;
+  if (mode == MDN_MODE_STEP && !jobs && nb > 0 && nb < n && Cb > 0 && nb * Cb + C <= h->num_sms) {
+    /* the nb largest replicas (the head of the largest-first order) on
+     * clusters of Cb CTAs, one cluster each, on the second stream; the rest
+     * on the SMs left.  The two launches share no replica. */
+    if ((e = cudaEventRecord(h->ev_fork, h->stream)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(h->stream2, h->ev_fork, 0)) != cudaSuccess ||
+        (e = launch_one(h, a, J.data(), nb, Cb, nb, h->job_order2, h->job_counter2, h->stream2)) != cudaSuccess ||
+        (e = launch_one(h, a, J.data() + nb, n - nb, C, (h->num_sms - nb * Cb) / C, h->job_order, h->job_counter,
+                        h->stream)) != cudaSuccess ||
+        (e = cudaEventRecord(h->ev_join, h->stream2)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(h->stream, h->ev_join, 0)) != cudaSuccess) {
+      *rc = fail(MDN_ERR_CUDA, "kernel launch: %s", cudaGetErrorString(e));
+      return 0;
+    }
+    return 2;
+  }
+  if ((e = launch_one(h, a, J.data(), n, C, h->num_sms / C, h->job_order, h->job_counter, h->stream)) !=
+      cudaSuccess) {
     *rc = fail(MDN_ERR_CUDA, "kernel launch: %s", cudaGetErrorString(e));
     return 0;
   }
@@ -680,6 +712,8 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
   ALLOC(h->status, R);
   ALLOC(h->job_order, R);
   ALLOC(h->job_counter, 1);
+  ALLOC(h->job_order2, R);
+  ALLOC(h->job_counter2, 1);
   ALLOC(h->d_ctl_mode, R);
   ALLOC(h->d_ctl_T, R);
 #undef ALLOC
@@ -688,6 +722,9 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
     if (e != cudaSuccess && rc == MDN_OK) rc = fail(MDN_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
   };
   ck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
+  ck(cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking), "stream");
+  ck(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming), "event");
+  ck(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming), "event");
   ck(cudaEventCreate(&h->ev0), "event");
   ck(cudaEventCreate(&h->ev1), "event");
   for (auto kern : {mdn_advance, mdn_advance_fp64}) {
@@ -1340,8 +1377,48 @@ int mdn_tune_launch(mdn_handle* h, long long n_steps, int* best) {
     }
   }
   h->opt.cluster_size = best_c;
+  /* then the largest replicas on clusters twice as large, beside the rest */
+  const int save_n = h->split_n, save_c = h->split_cluster;
+  int best_n = 0;
+  if (save_n == 0 && 2 * best_c <= 8)
+    for (int k = 2; k <= 8 && k < h->R; k *= 2) {
+      if (k * 2 * best_c + best_c > h->num_sms) break;
+      h->split_n = k;
+      h->split_cluster = 2 * best_c;
+      int rc = mdn_step(h, n_steps, 0);
+      if (rc == MDN_ERR_REPLICA) status = rc;
+      else if (rc != MDN_OK) {
+        h->split_n = save_n;
+        h->split_cluster = save_c;
+        return rc;
+      }
+      if (h->last_ms < best_ms) {
+        best_n = k;
+        best_ms = h->last_ms;
+      }
+    }
+  if (save_n == 0) {
+    h->split_n = best_n;
+    h->split_cluster = best_n ? 2 * best_c : 0;
+  }
   if (best) *best = best_c;
   return status;
+}
+
+int mdn_set_split(mdn_handle* h, int n_largest, int cluster_size) {
+  if (!h) return fail(MDN_ERR_ARG, "null handle");
+  if (n_largest < 0 || (n_largest > 0 && (cluster_size < 1 || cluster_size > 8)))
+    return fail(MDN_ERR_ARG, "split: n_largest >= 0 and cluster size 1..8");
+  h->split_n = n_largest;
+  h->split_cluster = n_largest ? cluster_size : 0;
+  return MDN_OK;
+}
+
+int mdn_get_split(mdn_handle* h, int* n_largest, int* cluster_size) {
+  if (!h) return fail(MDN_ERR_ARG, "null handle");
+  if (n_largest) *n_largest = h->split_n;
+  if (cluster_size) *cluster_size = h->split_cluster;
+  return MDN_OK;
 }
 
 int mdn_set_launch(mdn_handle* h, int cluster_size, int threads, int steps_per_launch) {

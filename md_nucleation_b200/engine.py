@@ -63,6 +63,8 @@ def lib():
         L.mdn_set_launch.argtypes = [vp, C.c_int, C.c_int, C.c_int]
         L.mdn_get_launch.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.mdn_tune_launch.argtypes = [vp, C.c_longlong, C.POINTER(C.c_int)]
+        L.mdn_set_split.argtypes = [vp, C.c_int, C.c_int]
+        L.mdn_get_split.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.mdn_adjoint_params.argtypes = [C.POINTER(abi.ReplicaDesc), C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int]
         L.mdn_adjoint.argtypes = [vp, C.POINTER(abi.ReplicaDesc), C.POINTER(abi.AdjointSpec),
                                   C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -224,11 +226,23 @@ class Engine:
         return c.value, t.value, n.value
 
     def tune_launch(self, n_steps: int = 100) -> int:
-        """Runs n_steps at each cluster size 1, 2, 4, 8 and keeps the fastest
-        (mdn_tune_launch); returns it.  The steps advance the replicas."""
+        """Runs n_steps at each cluster size 1, 2, 4, 8 and keeps the fastest,
+        then tries the split launch (mdn_tune_launch); returns the cluster
+        size.  The steps advance the replicas."""
         best = C.c_int(0)
         _ck(self.L.mdn_tune_launch(self.h, n_steps, C.byref(best)))
         return best.value
+
+    def set_split(self, n_largest: int, cluster_size: int = 0):
+        """The n_largest replicas in a concurrent second launch on clusters of
+        cluster_size CTAs (mdn_set_split); 0 turns it off."""
+        _ck(self.L.mdn_set_split(self.h, n_largest, cluster_size))
+
+    def get_split(self):
+        """(n_largest, cluster_size) of the split launch, (0, 0) when off."""
+        n, c = C.c_int(), C.c_int()
+        _ck(self.L.mdn_get_split(self.h, C.byref(n), C.byref(c)))
+        return n.value, c.value
 
     # ---- gradient harness ------------------------------------------------------
     def adjoint_params(self):

@@ -197,6 +197,24 @@ def test_tuned_launch_keeps_the_trajectory(eng):
             assert np.array_equal(getattr(sa, name), getattr(sb, name)), name
 
 
+def test_split_launch_keeps_the_trajectory(eng):
+    """The two largest replicas in a concurrent second launch on clusters of 4
+    (mdn_set_split), the rest at 2: the states equal those of one launch."""
+    specs = [systems.make(n) for n in systems.ALL]
+    a = eng.Engine(specs, cluster_size=2)
+    b = eng.Engine(specs, cluster_size=2)
+    b.set_split(2, 4)
+    assert b.get_split() == (2, 4)
+    a.step(40)
+    b.step(40)
+    _, launches = b.last_timing()
+    assert launches == 2
+    for r, spec in enumerate(specs):
+        compare_states(a.state(r), b.state(r), spec, 0.0, 0.0)
+    b.set_split(0)
+    assert b.get_split() == (0, 0)
+
+
 def test_steps_per_launch_invariance(eng):
     spec = systems.make("nacl_n2rigid_water")
     e0 = eng.Engine([spec])
