@@ -450,7 +450,8 @@ def run_engine(args):
     free0, total = torch.cuda.mem_get_info(device)
     checked = abi.Q_ALL & ~abi.Q_BLIND_INSERT
     t0 = time.time()
-    eng = engine.Engine(specs, quirks=checked, device=local, use_graph=1)
+    eng = engine.Engine(specs, quirks=checked, device=local, use_graph=1,
+                        **({"threads": args.threads} if args.threads else {}))
     free1, _ = torch.cuda.mem_get_info(device)
     resident = free0 - free1
     log(f"rank {rank}: engine created in {time.time() - t0:.1f} s, {resident / 2**30:.2f} GiB resident")
@@ -632,6 +633,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the gradient-harness measurement")
     ap.add_argument("--no-placement", action="store_true", help="skip the initial-placement measurement")
     ap.add_argument("--cluster", type=int, default=0, help="CTAs per replica (1..8); 0 = tuned in the warm-up")
+    ap.add_argument("--threads", type=int, default=0, help="threads per CTA (multiple of 32, <= 512); 0 = 512")
     ap.add_argument("--split", type=int, default=0,
                     help="with --cluster: the N largest replicas on clusters twice as large, in a concurrent launch")
     args = ap.parse_args()
