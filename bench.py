@@ -636,11 +636,17 @@ def main():
     ap.add_argument("--threads", type=int, default=0, help="threads per CTA (multiple of 32, <= 512); 0 = 512")
     ap.add_argument("--split", type=int, default=0,
                     help="with --cluster: the N largest replicas on clusters twice as large, in a concurrent launch")
+    ap.add_argument("--only-placement", action="store_true",
+                    help="print only the initial-placement measurement (mdn_place on configuration 4)")
     args = ap.parse_args()
     if args.warmup < 3 and not os.environ.get("MDN_BENCH_ALLOW_SHORT"):
         raise SystemExit("bench.py: --warmup must be >= 3")
     if args.impl == "reference":
         return run_reference(args)
+    if args.only_placement:
+        from md_nucleation_b200 import engine
+        print(json.dumps(placement_measurement(engine)))
+        return 0
     return run_engine(args)
 
 
