@@ -227,7 +227,10 @@ int place_species(Dev& d, const mdn_place_desc* p, uint32_t species, long long n
       snprintf(msg, sizeof msg, "%s placement did not converge (box %.1f A)", what, p->box);
       return mdn_error(MDN_ERR_ARG, msg);
     }
-    const int K = (int)std::min<long long>(chunk, cap - k0);
+    /* candidates this round: the molecules still wanted plus a quarter
+     * (the acceptance is near 1 in the reference's dilute boxes) */
+    const long long want = n - placed;
+    const int K = (int)std::min(std::min<long long>(chunk, want + want / 4 + 4096), cap - k0);
     const int big = INT_MAX;
     if ((e = cudaMemcpyAsync(d.first, &big, sizeof(int), cudaMemcpyHostToDevice, d.st)) != cudaSuccess)
       return cuda_fail("copy", e);
@@ -285,8 +288,7 @@ extern "C" int mdn_place(int device, const mdn_place_desc* p, double* gas_x, dou
   if (e != cudaSuccess) return cuda_fail("cudaSetDevice", e);
   const long long nmax = std::max(p->n_gas, p->n_vapor);
   if (nmax == 0) return MDN_OK;
-  /* candidates per round: the molecules still wanted plus a quarter (the
-   * acceptance is near 1 in the reference's dilute boxes) */
+  /* the largest round either species can take */
   const long long chunk = std::min<long long>(nmax + nmax / 4 + 4096, 1LL << 26);
   Dev d;
   if ((e = cudaStreamCreateWithFlags(&d.st, cudaStreamNonBlocking)) != cudaSuccess ||
