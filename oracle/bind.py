@@ -26,6 +26,14 @@ _ref = None
 _orc = None
 
 
+# where oracle/Makefile reads the reference's sources (its REF variable)
+REF_SRC = os.path.join(os.environ.get("REF", "/root/reference"), "src")
+
+
+def reference_sources_present() -> bool:
+    return os.path.isdir(REF_SRC)
+
+
 def build(reference: bool = True):
     """Runs oracle/Makefile (the reference part only if its sources are present)."""
     target = "all" if reference else "restatement"

@@ -19,8 +19,8 @@ def oracle_libs():
     only where the reference sources exist)."""
     from oracle import bind
     if not os.path.exists(bind.ORC_LIB) or (
-            os.path.isdir("/root/reference/src") and not os.path.exists(bind.REF_LIB)):
-        bind.build(reference=os.path.isdir("/root/reference/src"))
+            bind.reference_sources_present() and not os.path.exists(bind.REF_LIB)):
+        bind.build(reference=bind.reference_sources_present())
     return bind
 
 
