@@ -42,7 +42,8 @@ extern "C" {
 /* ---- per-replica status bits (mdn_get_status) ---------------------------- */
 #define MDN_ST_SLAB_OVERFLOW   0x0001 /* more in-domain gas molecules than the slab holds */
 #define MDN_ST_CORE_OVERFLOW   0x0002 /* more in-domain vapor atoms than the core holds */
-#define MDN_ST_LIST_OVERFLOW   0x0004 /* gas-ion / gas-vapor / gas-gas pair list full */
+#define MDN_ST_LIST_OVERFLOW   0x0004 /* gas-ion / gas-vapor / gas-gas pair list full
+                                         (at most 64,511 gas molecules with list entries) */
 #define MDN_ST_SHAKE_NOCONV    0x0008 /* SHAKE hit its iteration cap */
 #define MDN_ST_NONFINITE       0x0010 /* a non-finite force, position or velocity */
 #define MDN_ST_FIXED_OVERFLOW  0x0020 /* a force left the 64-bit fixed-point range */
