@@ -422,7 +422,7 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "replicas": args.replicas, "md_steps_per_step": MD_STEPS,
-                   "path": "reference routines (MD::verlet, SHAKE step where set) compiled from the "
+                   "path": "reference routines (MD::verlet as shipped, which never calls SHAKE) compiled from the "
                            "reference sources, one replica per OpenMP thread"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                          "sample": sample},
