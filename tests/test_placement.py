@@ -140,3 +140,17 @@ def test_host_cpu_placement_rule(tmp_path):
         assert min_image_dist(X, ion, d.box).min() > 10.0
     assert np.all(np.sqrt((gx[1:] ** 2).sum(1)) > 10.0)
     assert np.all(np.sqrt((vx ** 2).sum(1)) > 10.0)
+
+
+def test_gpu_placement_fails_loudly_without_a_gpu(tmp_path):
+    """mdn_place and the host's GPU placement report the missing device."""
+    from md_nucleation_b200 import build, engine
+    build.build()
+    if engine.device_count() > 0:
+        pytest.skip("a GPU is present (tests/test_gpu_placement.py runs the placement)")
+    with pytest.raises(engine.MdnError, match="no CUDA device"):
+        engine.place(100.0, np.zeros((1, 3)), 10, 0, 300.0, 300.0, 1)
+    from md_nucleation_b200 import host as H
+    from tests.test_host import write_case
+    with pytest.raises(H.HostError, match="no CUDA device"):
+        H.HostSystem(write_case(tmp_path, "nacl"), calc_number=1, place_device=0)
