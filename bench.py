@@ -638,6 +638,8 @@ def main():
                     help="with --cluster: the N largest replicas on clusters twice as large, in a concurrent launch")
     ap.add_argument("--only-placement", action="store_true",
                     help="print only the initial-placement measurement (mdn_place on configuration 4)")
+    ap.add_argument("--only-adjoint", action="store_true",
+                    help="print only the gradient-harness measurement (mdn_adjoint on configuration 1)")
     args = ap.parse_args()
     if args.warmup < 3 and not os.environ.get("MDN_BENCH_ALLOW_SHORT"):
         raise SystemExit("bench.py: --warmup must be >= 3")
@@ -646,6 +648,10 @@ def main():
     if args.only_placement:
         from md_nucleation_b200 import engine
         print(json.dumps(placement_measurement(engine)))
+        return 0
+    if args.only_adjoint:
+        from md_nucleation_b200 import engine
+        print(json.dumps(adjoint_measurement(engine)))
         return 0
     return run_engine(args)
 
