@@ -632,8 +632,8 @@ __device__ __forceinline__ double charge_d(const Ctx& x, int i) {
 /* forces of the core (ion + vapor) among themselves, and the core kick        */
 /* ------------------------------------------------------------------------- */
 /* One term of the core force sums.  Each 64-bit fixed-point term
- * u = lo16 + 2^16 mid16 + 2^32 hi32 goes into three 32-bit sums (32-bit
- * shared-memory atomics are native, 64-bit ones are not).  The two 16-bit
+ * u = lo16 + 2^16 mid16 + 2^32 hi32 goes into three 32-bit sums (64-bit
+ * shared-memory atomics measured far slower than 32-bit ones here).  The two 16-bit
  * sums are exact for up to 65,536 terms per atom and evaluation (one per
  * near gas molecule, whose list holds at most 64,511, plus at most one per
  * pair tile and per bonded term); the high sum only matters modulo 2^32.
