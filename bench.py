@@ -248,7 +248,11 @@ class stdout_to_stderr:
 
 
 def _cpu_sample_child(specs, threads, budget_s, q):
+    import tempfile
     from oracle import bind
+    # the reference's make_pair appends vapor in/out logs to the working
+    # directory (src/output/output.cpp:44-65): keep them out of the tree
+    os.chdir(tempfile.mkdtemp(prefix="mdn_ref_sample_"))
     with stdout_to_stderr():
         reps = [bind.RefReplica(sp) for sp in specs]
     t0 = time.perf_counter()

@@ -304,13 +304,14 @@ int  mdn_snapshot(mdn_handle* h, long long* offset, long long capacity, int* typ
  * handed all free device memory to its own pool, or that runs under a fixed
  * device-memory budget, cannot let a dump taken late in a run allocate, or
  * fail for lack of memory.  This call stages the rows in a fixed array that
- * the library holds on each device from the moment it is loaded there:
+ * the library holds on each device until the process exits:
  * MDN_NOALLOC_MAX_ROWS rows (52 bytes each) and MDN_NOALLOC_MAX_REPLICAS
  * replicas, 3.4 MB in all.  A larger snapshot, or a larger batch, returns
  * MDN_ERR_CAPACITY and says so in mdn_last_error (offset filled when the
- * replica count fits); use mdn_snapshot for those.  The first call on a
- * device looks the array up on that device (once per device per process);
- * make that first call before any stream capture.  Every call in the process
+ * replica count fits); use mdn_snapshot for those.  The first mdn_create on
+ * a device is where the array is loaded (and its 3.4 MB allocated) and
+ * looked up, together with the snapshot kernels, once per device per
+ * process; this call itself then loads nothing.  Every call in the process
  * shares the one array per device: calls that overlap in time on the same
  * device, from different threads or handles, race and may return each
  * other's rows.  Nothing in the array has to start at zero: each call writes

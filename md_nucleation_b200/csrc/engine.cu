@@ -26,10 +26,11 @@
 
 extern "C" __global__ void mdn_advance(KArgs a);
 extern "C" __global__ void mdn_advance_fp64(KArgs a);
-int mdn_snapshot_device(const RepParams* dP, const RepDyn* dD, const int* d_iblob, int R, const double* ion_x,
-                        const double* ion_v, const double* slab_x, const double* slab_v, const double* vslab_x,
-                        const double* vslab_v, long long* d_offset, int* d_type, double* d_x, double* d_v,
-                        long long d_capacity, cudaStream_t stream);
+cudaError_t mdn_snapshot_device(const RepParams* dP, const RepDyn* dD, const int* d_iblob, int R,
+                                const double* ion_x, const double* ion_v, const double* slab_x,
+                                const double* slab_v, const double* vslab_x, const double* vslab_v,
+                                long long* d_offset, int* d_type, double* d_x, double* d_v, long long d_capacity,
+                                cudaStream_t stream);
 
 namespace {
 
@@ -330,6 +331,8 @@ __attribute__((visibility("hidden"))) void mdn_snapshot_args(const mdn_handle* h
 }
 
 __attribute__((visibility("hidden"))) int mdn_error(int code, const char* msg) { return fail(code, "%s", msg); }
+
+__attribute__((visibility("hidden"))) void mdn_noalloc_setup(int dev);
 
 __attribute__((visibility("hidden"))) unsigned mdn_internal_quirks(const mdn_handle* h) { return h->opt.quirks; }
 
@@ -794,6 +797,9 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
     delete h;
     return rc;
   }
+  /* the allocation-free snapshot's per-device set-up (snapshot_noalloc.cu):
+   * its fixed array and kernels are loaded here, not by its first call */
+  mdn_noalloc_setup(h->dev);
   *out = h;
   return MDN_OK;
 }
@@ -1233,9 +1239,10 @@ int mdn_snapshot(mdn_handle* h, long long* offset, long long capacity, int* type
     CK(cudaMalloc((void**)&h->snap_x, 3 * sizeof(double) * std::max<long long>(cap, 1)));
     CK(cudaMalloc((void**)&h->snap_v, 3 * sizeof(double) * std::max<long long>(cap, 1)));
   }
-  if (mdn_snapshot_device(h->dP, h->dD, h->d_iblob, h->R, h->ion_x, h->ion_v, h->slab_x, h->slab_v, h->vslab_x,
-                          h->vslab_v, h->snap_off, h->snap_type, h->snap_x, h->snap_v, h->snap_cap, h->stream))
-    return fail(MDN_ERR_CUDA, "snapshot kernels: %s", cudaGetErrorString(cudaGetLastError()));
+  const cudaError_t le = mdn_snapshot_device(h->dP, h->dD, h->d_iblob, h->R, h->ion_x, h->ion_v, h->slab_x,
+                                             h->slab_v, h->vslab_x, h->vslab_v, h->snap_off, h->snap_type, h->snap_x,
+                                             h->snap_v, h->snap_cap, h->stream);
+  if (le != cudaSuccess) return fail(MDN_ERR_CUDA, "snapshot kernels: %s", cudaGetErrorString(le));
   CK(cudaMemcpyAsync(offset, h->snap_off, sizeof(long long) * (h->R + 1), cudaMemcpyDeviceToHost, h->stream));
   std::vector<long long> e(U ? 8 * h->R : 0);
   if (U) CK(cudaMemcpyAsync(e.data(), h->energy, sizeof(long long) * e.size(), cudaMemcpyDeviceToHost, h->stream));

@@ -77,13 +77,26 @@ __global__ void snapshot_gather(const RepParams* P, const RepDyn* D, const int* 
 
 }  // namespace
 
-/* Host side, called from engine.cu with the handle's device pointers. */
-int mdn_snapshot_device(const RepParams* dP, const RepDyn* dD, const int* d_iblob, int R, const double* ion_x,
-                        const double* ion_v, const double* slab_x, const double* slab_v, const double* vslab_x,
-                        const double* vslab_v, long long* d_offset, int* d_type, double* d_x, double* d_v,
-                        long long d_capacity, cudaStream_t stream) {
+/* Host side, called from engine.cu and snapshot_noalloc.cu with the
+ * handle's device pointers.  Returns the launch error it read (and thereby
+ * cleared), cudaSuccess when both kernels were queued. */
+cudaError_t mdn_snapshot_device(const RepParams* dP, const RepDyn* dD, const int* d_iblob, int R,
+                                const double* ion_x, const double* ion_v, const double* slab_x,
+                                const double* slab_v, const double* vslab_x, const double* vslab_v,
+                                long long* d_offset, int* d_type, double* d_x, double* d_v, long long d_capacity,
+                                cudaStream_t stream) {
   snapshot_counts<<<1, 32, 0, stream>>>(dP, dD, R, d_offset);
   snapshot_gather<<<R, 256, 0, stream>>>(dP, dD, d_iblob, d_offset, d_capacity, ion_x, ion_v, slab_x, slab_v,
                                          vslab_x, vslab_v, d_type, d_x, d_v);
-  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+  return cudaGetLastError();
+}
+
+/* Loads the snapshot kernels on the current device (under lazy module
+ * loading a kernel's module is loaded, and its code memory allocated, when
+ * the kernel is first named), so that a later snapshot loads nothing. */
+__attribute__((visibility("hidden"))) cudaError_t mdn_snapshot_load_kernels() {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, snapshot_counts);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, snapshot_gather);
+  return e;
 }

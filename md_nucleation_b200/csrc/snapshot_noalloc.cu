@@ -15,6 +15,12 @@
  * 0..R, snapshot_gather writes every row below offset[R] (and none at or
  * beyond MDN_NOALLOC_MAX_ROWS), and only those are copied back.  Every call
  * in the process shares it; calls that overlap in time on one device race.
+ *
+ * The per-device set-up (the array's device address, found with
+ * cudaGetSymbolAddress; the module that holds the array, and the snapshot
+ * kernels' module, loaded) runs once per device inside mdn_create, so even
+ * under lazy module loading the first snapshot call loads and allocates
+ * nothing.
  */
 #include <cuda_runtime.h>
 #include <stdio.h>
@@ -25,12 +31,14 @@
 #include "mdn.h"
 #include "mdn_types.h"
 
-int mdn_snapshot_device(const RepParams* dP, const RepDyn* dD, const int* d_iblob, int R, const double* ion_x,
-                        const double* ion_v, const double* slab_x, const double* slab_v, const double* vslab_x,
-                        const double* vslab_v, long long* d_offset, int* d_type, double* d_x, double* d_v,
-                        long long d_capacity, cudaStream_t stream);
+cudaError_t mdn_snapshot_device(const RepParams* dP, const RepDyn* dD, const int* d_iblob, int R,
+                                const double* ion_x, const double* ion_v, const double* slab_x,
+                                const double* slab_v, const double* vslab_x, const double* vslab_v,
+                                long long* d_offset, int* d_type, double* d_x, double* d_v, long long d_capacity,
+                                cudaStream_t stream);
 __attribute__((visibility("hidden"))) void mdn_snapshot_args(const mdn_handle* h, SnapshotArgs* s);
 __attribute__((visibility("hidden"))) int mdn_error(int code, const char* msg);
+__attribute__((visibility("hidden"))) cudaError_t mdn_snapshot_load_kernels();
 
 namespace {
 
@@ -61,17 +69,26 @@ int error(int code, const char* fmt, long long a, long long b) {
   return mdn_error(code, buf);
 }
 
-/* The device address of the array on `dev` (current device), looked up on
- * the first call for that device. */
+/* The per-device set-up, once per device with that device current: the
+ * device address of the array (looking it up loads the module that holds
+ * it, which is where the array's memory is allocated), and the snapshot
+ * kernels loaded too.  mdn_create runs it for its device, so a snapshot
+ * call finds it done. */
+void setup_once(int dev) {
+  std::call_once(g_once[dev], [dev] {
+    void* p = nullptr;
+    g_setup_rc[dev] = cudaGetSymbolAddress(&p, g_snapshot_scratch);
+    if (g_setup_rc[dev] == cudaSuccess) g_setup_rc[dev] = mdn_snapshot_load_kernels();
+    g_scratch[dev] = g_setup_rc[dev] == cudaSuccess ? (unsigned char*)p : nullptr;
+  });
+}
+
+/* The device address of the array on `dev` (current device). */
 int scratch_on(int dev, unsigned char** out) {
   if (dev < 0 || dev >= MAX_DEVICES)
     return error(MDN_ERR_ARG, "mdn_snapshot_noalloc: device %lld beyond the %lld devices it supports", dev,
                  MAX_DEVICES);
-  std::call_once(g_once[dev], [dev] {
-    void* p = nullptr;
-    g_setup_rc[dev] = cudaGetSymbolAddress(&p, g_snapshot_scratch);
-    g_scratch[dev] = g_setup_rc[dev] == cudaSuccess ? (unsigned char*)p : nullptr;
-  });
+  setup_once(dev);
   if (g_setup_rc[dev] != cudaSuccess || !g_scratch[dev]) {
     char buf[256];
     snprintf(buf, sizeof buf, "mdn_snapshot_noalloc: cudaGetSymbolAddress of the staging array failed: %s",
@@ -89,6 +106,13 @@ int cuda_fail(const char* what, cudaError_t e) {
 }
 
 }  // namespace
+
+/* Internal, for mdn_create: the set-up above for the handle's device (the
+ * current device).  A failure is kept and reported by mdn_snapshot_noalloc,
+ * so creating a handle never fails for it. */
+__attribute__((visibility("hidden"))) void mdn_noalloc_setup(int dev) {
+  if (dev >= 0 && dev < MAX_DEVICES) setup_once(dev);
+}
 
 extern "C" int mdn_snapshot_noalloc(mdn_handle* h, long long* offset, long long capacity, int* type, double* x,
                                     double* v, double* U) {
@@ -110,9 +134,9 @@ extern "C" int mdn_snapshot_noalloc(mdn_handle* h, long long* offset, long long 
   int* d_type = (int*)(base + TYPE_AT);
   double* d_x = (double*)(base + X_AT);
   double* d_v = (double*)(base + V_AT);
-  if (mdn_snapshot_device(s.P, s.D, s.iblob, s.R, s.ion_x, s.ion_v, s.slab_x, s.slab_v, s.vslab_x, s.vslab_v, d_off,
-                          d_type, d_x, d_v, (long long)ROWS, st))
-    return cuda_fail("snapshot kernels", cudaGetLastError());
+  if ((e = mdn_snapshot_device(s.P, s.D, s.iblob, s.R, s.ion_x, s.ion_v, s.slab_x, s.slab_v, s.vslab_x,
+                               s.vslab_v, d_off, d_type, d_x, d_v, (long long)ROWS, st)) != cudaSuccess)
+    return cuda_fail("snapshot kernels", e);
   if ((e = cudaMemcpyAsync(offset, d_off, sizeof(long long) * (s.R + 1), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
     return cuda_fail("offset copy", e);
   /* energies: the int64 fixed-point sums land in U itself and are converted

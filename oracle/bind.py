@@ -26,8 +26,9 @@ _ref = None
 _orc = None
 
 
-# where oracle/Makefile reads the reference's sources (its REF variable)
-REF_SRC = os.path.join(os.environ.get("REF", "/root/reference"), "src")
+# where oracle/Makefile reads the reference's sources: its REF variable from
+# the environment, else the reference checkout beside the repository
+REF_SRC = os.path.join(os.environ.get("REF", os.path.join(os.path.dirname(HERE), "..", "reference")), "src")
 
 
 def reference_sources_present() -> bool:

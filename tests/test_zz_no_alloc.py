@@ -66,6 +66,27 @@ def same(got, buf):
     assert np.array_equal(U, buf.U)
 
 
+def test_noalloc_allocates_no_device_memory(eng):
+    """The point of the entry point: on a handle that never took a
+    mdn_snapshot, neither the first nor the second call takes device memory
+    (the fixed array and the snapshot kernels are loaded by mdn_create).
+    Free device memory is read with cudaMemGetInfo through torch."""
+    import torch
+    torch.cuda.init()
+    e = eng.Engine([systems.make("chain_he_water"), systems.make("nacl_n2_meoh")])
+    e.step(4, energy_mode=1)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    first = noalloc(e, MAX_ROWS)
+    free1, _ = torch.cuda.mem_get_info(0)
+    second = noalloc(e, MAX_ROWS)
+    free2, _ = torch.cuda.mem_get_info(0)
+    assert first[0] == 0 and second[0] == 0
+    assert free1 >= free0, f"the first call took {free0 - free1} bytes of device memory"
+    assert free2 >= free0, f"the second call took {free0 - free2} bytes of device memory"
+    assert np.array_equal(first[1], second[1]) and np.array_equal(first[3], second[3])
+
+
 def test_noalloc_matches_snapshot_twice_in_a_row(eng):
     specs = [systems.make(n) for n in ("nacl_n2_meoh", "chain_he_water", "nacl_n2mono_meoh")]
     e = eng.Engine(specs)
