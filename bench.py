@@ -56,15 +56,24 @@ def _make_replica(r):
     return generate.config2_replica(r)
 
 
-def make_specs(first: int, n: int, workers: int):
-    """Generates the replicas in a spawn pool (the chain growth and the
-    placement of up to 100,000 molecules take seconds per replica)."""
+def make_specs(first: int, n: int, workers: int, indices=None):
+    """Generates the replicas first..first+n-1 (or the listed indices) in a
+    spawn pool (the chain growth and the placement of up to 100,000
+    molecules take seconds per replica)."""
     t0 = time.time()
+    idx = list(indices) if indices is not None else list(range(first, first + n))
     ctx = mp.get_context("spawn")
-    with ctx.Pool(max(1, workers)) as pool:
-        specs = pool.map(_make_replica, range(first, first + n), chunksize=1)
-    log(f"generated {n} replicas in {time.time() - t0:.1f} s on {workers} workers")
+    with ctx.Pool(max(1, min(workers, len(idx)))) as pool:
+        specs = pool.map(_make_replica, idx, chunksize=1)
+    log(f"generated {len(idx)} replicas in {time.time() - t0:.1f} s on {workers} workers")
     return specs
+
+
+def sample_indices(n_replicas: int, threads: int):
+    """The replicas the CPU samples run: 2 per host thread, spread evenly
+    over the batch."""
+    stride = max(1, n_replicas // (2 * threads))
+    return list(range(0, n_replicas, stride))[:2 * threads], stride
 
 
 def in_domain_atoms(infos, specs):
@@ -247,7 +256,7 @@ class stdout_to_stderr:
         os.close(self.saved)
 
 
-def _cpu_sample_child(specs, threads, budget_s, q):
+def _cpu_sample_child(specs, threads, budget_s, n_samples, q):
     import tempfile
     from oracle import bind
     # the reference's make_pair appends vapor in/out logs to the working
@@ -259,40 +268,43 @@ def _cpu_sample_child(specs, threads, budget_s, q):
     bind.ref_verlet_many(reps, 5, threads)
     cal = (time.perf_counter() - t0) / 5
     n = max(5, int(budget_s / max(cal, 1e-6)))
-    atoms0 = sum(r.in_domain_atoms() for r in reps)
-    t0 = time.perf_counter()
-    bind.ref_verlet_many(reps, n, threads)
-    dt = time.perf_counter() - t0
-    atoms1 = sum(r.in_domain_atoms() for r in reps)
-    q.put((0.5 * (atoms0 + atoms1) * n / dt, n, atoms0, dt))
+    out = []
+    for _ in range(n_samples):
+        atoms0 = sum(r.in_domain_atoms() for r in reps)
+        t0 = time.perf_counter()
+        bind.ref_verlet_many(reps, n, threads)
+        dt = time.perf_counter() - t0
+        atoms1 = sum(r.in_domain_atoms() for r in reps)
+        out.append((0.5 * (atoms0 + atoms1) * n / dt, n, atoms0, dt))
+    q.put(out)
 
 
-def cpu_sample(specs, threads: int, budget_s: float):
-    """Times the reference's MD::verlet on `2 * threads` replicas spread over
-    the batch, one replica per OpenMP thread at a time (src/main.cpp:22-29);
-    returns (atom-steps/s, what was sampled), or (None, reason).  The step
-    count is sized from a 5-step calibration so the sample takes about
-    `budget_s`; the sample runs in a child process that is ended after
-    3 * budget_s + 120 s."""
+def cpu_samples(specs, n_total: int, stride: int, threads: int, budget_s: float, n_samples: int = 1):
+    """Times the reference's MD::verlet on the sampled replicas `specs`, one
+    replica per OpenMP thread at a time (src/main.cpp:22-29), in
+    `n_samples` consecutive samples of about `budget_s` each (the step
+    count is sized from a 5-step calibration); the replicas are built once
+    in a child process, which is ended after n_samples * 3 * budget_s + 120 s.
+    Returns ([atom-steps/s per sample], what was sampled) or (None, reason)."""
     ctx = mp.get_context("spawn")
-    stride = max(1, len(specs) // (2 * threads))
-    pick = [specs[r] for r in list(range(0, len(specs), stride))[:2 * threads]]
     q = ctx.Queue()
-    p = ctx.Process(target=_cpu_sample_child, args=(pick, threads, budget_s, q))
+    p = ctx.Process(target=_cpu_sample_child, args=(specs, threads, budget_s, n_samples, q))
     p.start()
-    limit = 3 * budget_s + 120
+    limit = n_samples * 3 * budget_s + 120
     try:
-        value, n, atoms, dt = q.get(timeout=limit)
-        sample = (f"{len(pick)} of the {len(specs)} replicas (every {stride}th), {n} MD steps each "
+        out = q.get(timeout=limit)
+        n, atoms, dt = out[-1][1], out[-1][2], out[-1][3]
+        values = [o[0] for o in out]
+        sample = (f"{len(specs)} of the {n_total} replicas (every {stride}th), {n} MD steps each per sample "
                   f"(MD::verlet as shipped: X-H bonds unconstrained, no SHAKE), {atoms} in-domain "
                   f"atoms, {dt:.1f} s wall on {threads} threads")
     except Exception:
-        value, sample = None, f"the reference sample did not finish within {limit:.0f} s"
+        values, sample = None, f"the reference sample did not finish within {limit:.0f} s"
     p.join(timeout=10)
     if p.is_alive():
         p.kill()
         p.join()
-    return value, sample
+    return values, sample
 
 
 def plain_sample(engine, specs, quirks, n_pick: int):
@@ -409,17 +421,16 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_harness.so was not built"}))
         return 0
     threads = host_threads()
-    specs = make_specs(0, args.replicas, threads)
-    values = []
-    sample = ""
-    for k in range(args.warmup + args.steps):
-        v, sample = cpu_sample(specs, threads, args.ref_budget)
-        if v is None:
-            print(json.dumps({"impl": "reference", "unavailable": sample}))
-            return 0
-        if k >= args.warmup:
-            values.append(v)
-        log(f"reference step {k}: {v:.4g} atom-steps/s ({sample})")
+    pick, stride = sample_indices(args.replicas, threads)
+    specs = make_specs(0, 0, threads, indices=pick)
+    values, sample = cpu_samples(specs, args.replicas, stride, threads, args.ref_budget,
+                                 args.warmup + args.steps)
+    if values is None:
+        print(json.dumps({"impl": "reference", "unavailable": sample}))
+        return 0
+    for k, v in enumerate(values):
+        log(f"reference step {k}: {v:.4g} atom-steps/s")
+    values = values[args.warmup:]
     value = float(np.mean(values))
     out = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
@@ -469,44 +480,66 @@ def run_engine(args):
     # warm-up: the launch-shape tuner (a block of MD_STEPS per cluster size,
     # then up to 3 blocks of split launches; results do not depend on the
     # shape), then the warm-up steps
+    def step_block(n, energy_mode=0):
+        """n MD steps; a replica that raises a fatal status is frozen by the
+        engine (mdn_step returns MDN_ERR_REPLICA) and counted below instead
+        of ending the run"""
+        try:
+            eng.step(n, energy_mode)
+        except engine.MdnError as ex:
+            if ex.code != abi.ERR_REPLICA:
+                raise
+
     if args.cluster:
         eng.set_launch(args.cluster)
         eng.set_split(args.split, 2 * args.cluster if args.split else 0)
         chosen_by = "--cluster / --split"
     else:
-        tuned = eng.tune_launch(MD_STEPS)
+        try:
+            tuned = eng.tune_launch(MD_STEPS)
+        except engine.MdnError as ex:
+            if ex.code != abi.ERR_REPLICA:
+                raise
+            tuned = eng.get_launch()[0]
         chosen_by = "mdn_tune_launch during warm-up"
         log(f"rank {rank}: tuned cluster size {tuned}")
     for _ in range(args.warmup):
-        eng.step(MD_STEPS)
+        step_block(MD_STEPS)
     barrier()
+    live0 = (eng.status() & abi.ST_FATAL) == 0
     infos0 = [eng.info(r) for r in range(eng.n)]
-    atoms0 = in_domain_atoms(infos0, specs)
-    flops0 = algorithmic_flops(infos0, specs)
     # timed region: K bench steps, device time from CUDA events on the
     # launching stream (mdn_last_timing)
     ms_total, launches = 0.0, 0
     barrier()
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
-            eng.step(MD_STEPS)
+            step_block(MD_STEPS)
             ms, nl = eng.last_timing()
             ms_total += ms
             launches += nl
         barrier()
     infos1 = [eng.info(r) for r in range(eng.n)]
-    atoms1 = in_domain_atoms(infos1, specs)
-    flops1 = algorithmic_flops(infos1, specs)
     status = eng.status()
     fatal = int(np.sum((status & abi.ST_FATAL) != 0))
     warned = int(np.sum((status != 0) & ((status & abi.ST_FATAL) == 0)))
+    # only replicas that advanced through the whole timed region count
+    live = live0 & ((status & abi.ST_FATAL) == 0)
+    keep = [r for r in range(eng.n) if live[r]]
+    infos0 = [infos0[r] for r in keep]
+    infos1 = [infos1[r] for r in keep]
+    kspecs = [specs[r] for r in keep]
+    atoms0 = in_domain_atoms(infos0, kspecs)
+    atoms1 = in_domain_atoms(infos1, kspecs)
+    flops0 = algorithmic_flops(infos0, kspecs)
+    flops1 = algorithmic_flops(infos1, kspecs)
     atom_steps = 0.5 * float(atoms0.sum() + atoms1.sum()) * MD_STEPS * args.steps
     ms_max = max_over_ranks(dist, ms_total, device)
     atom_steps_all = sum_over_ranks(dist, atom_steps, device)
     value = atom_steps_all / (ms_max * 1e-3)
     flops_per_md_step = 0.5 * (flops0 + flops1)
     achieved_tflops = flops_per_md_step * MD_STEPS * args.steps / (ms_total * 1e-3) / 1e12
-    bytes_timed = algorithmic_bytes(infos0, infos1, specs, MD_STEPS * args.steps)
+    bytes_timed = algorithmic_bytes(infos0, infos1, kspecs, MD_STEPS * args.steps)
     achieved_gbs = bytes_timed / (ms_total * 1e-3) / 1e9
     clocks = clk.summary()
 
@@ -517,12 +550,12 @@ def run_engine(args):
     temps = engine.PinnedArray((eng.n,), np.float64)
     modes.array[:] = [s.nvt_mode for s in specs]
     temps.array[:] = [s.nvt_temperature for s in specs]
-    cap = int(atoms1.max() * 1.5 * eng.n) + 1024
+    cap = int(in_domain_atoms([eng.info(r) for r in range(eng.n)], specs).max() * 1.5 * eng.n) + 1024
     snap = engine.SnapshotBuffer(eng.n, cap, pinned=True)
     e2e_steps = max(1, min(args.steps, 3))
     # one untimed pass loads the snapshot kernels and touches the host pages
     eng.set_nvt_batch(modes.array, temps.array)
-    eng.step(MD_STEPS, energy_mode=1)
+    step_block(MD_STEPS, energy_mode=1)
     eng.snapshot(snap, energies=True)
     barrier()
     t0 = time.perf_counter()
@@ -530,7 +563,7 @@ def run_engine(args):
     e2e_atom_steps = 0.0
     for _ in range(e2e_steps):
         eng.set_nvt_batch(modes.array, temps.array)
-        eng.step(MD_STEPS, energy_mode=1)
+        step_block(MD_STEPS, energy_mode=1)
         eng.snapshot(snap, energies=True)
         d2h += snap.nbytes_used + (eng.n + 1) * 8 + eng.n * 64
         e2e_atom_steps += float(snap.offset[-1]) * MD_STEPS
@@ -553,7 +586,7 @@ def run_engine(args):
             "config": {
                 "workload": WORKLOAD, "replicas_per_gpu": eng.n, "md_steps_per_step": MD_STEPS,
                 "in_domain_atoms_per_gpu": int(atoms1.sum()),
-                "in_domain_atoms_range": [int(atoms1.min()), int(atoms1.max())],
+                "in_domain_atoms_range": [int(atoms1.min()), int(atoms1.max())] if len(atoms1) else None,
                 "insertion": "checked (rotation re-drawn until no atom within 2 A)",
                 "l2": f"inputs larger than L2: {resident / 2**30:.2f} GiB resident per GPU",
                 "replicas_with_warnings": warned, "replicas_failed": fatal,
@@ -564,36 +597,39 @@ def run_engine(args):
                            "chosen_by": chosen_by},
             },
             "roofline": {
-                "bound": "hbm", "achieved": achieved_gbs, "peak": None, "unit": "GB/s", "frac": None,
-                "traffic": None, "kernel": "mdn_advance",
-                "algorithmic_bytes_per_launch": bytes_timed / args.steps,
-                "launch": f"{MD_STEPS} MD steps of every replica",
-                "fp32": {"achieved": achieved_tflops, "unit": "TFLOP/s",
-                         "algorithmic_flops_per_md_step": flops_per_md_step},
+                "bound": "fp32", "achieved": achieved_tflops, "peak": None, "unit": "TFLOP/s", "frac": None,
+                "traffic": None, "kernel": "mdn_advance", "launch": f"{MD_STEPS} MD steps of every replica",
+                "algorithmic_flops_per_launch": flops_per_md_step * MD_STEPS,
+                "hbm": {"achieved": achieved_gbs, "unit": "GB/s",
+                        "algorithmic_bytes_per_launch": bytes_timed / args.steps,
+                        "model": "streaming byte model: 204 B per in-domain atom-step, 4 B per list entry and "
+                                 "step, 72 B per molecule and rebuild"},
             },
             "gpu_launches": launches,
             "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d_per_step,
                     "d2h_bytes_per_step": int(d2h / e2e_steps)},
         }
+        # the kernel's bound is FP32 issue and latency, not DRAM (each
+        # replica's core sits in shared memory, its gas slab in L2): the
+        # headline fraction is the algorithmic pair flops against the FP32
+        # pipes, 148 SMs x 128 lanes x 2 flops (FMA) at the SM clock sampled
+        # during the timed region (no FP32 figure is measured separately on
+        # these GPUs); the byte model against the measured copy bandwidth is
+        # kept beside it
+        props = torch.cuda.get_device_properties(device)
+        mhz = clocks["sm_mhz"] or 1965.0
+        peak = props.multi_processor_count * 128 * 2 * mhz * 1e6 / 1e12
+        out["roofline"].update({"peak": peak, "frac": achieved_tflops / peak,
+                                "peak_source": f"{props.multi_processor_count} SMs x 128 FP32 lanes x 2 at the "
+                                               f"sampled median {mhz:.0f} MHz"})
         hbm, hbm_src = measured_hbm_peak()
-        out["roofline"]["peak"] = hbm
-        out["roofline"]["frac"] = achieved_gbs / hbm
-        out["roofline"]["peak_source"] = hbm_src
+        out["roofline"]["hbm"].update({"peak": hbm, "frac": achieved_gbs / hbm, "peak_source": hbm_src})
         # DRAM bytes of one launch from ncu (a 32-replica capture scaled by
         # atom-steps; profiles/mdn_advance_batched.md)
         traffic = traffic_per_atom_step()
         if traffic is not None:
             out["roofline"]["traffic"] = traffic * atom_steps / args.steps
-        # FP32 peak: 148 SMs x 128 FP32 lanes x 2 flops (FMA) at the SM clock
-        # measured during the timed region (no FP32 figure is measured
-        # separately on these GPUs)
-        props = torch.cuda.get_device_properties(device)
-        mhz = clocks["sm_mhz"] or 1965.0
-        peak = props.multi_processor_count * 128 * 2 * mhz * 1e6 / 1e12
-        out["roofline"]["fp32"].update({"peak": peak, "frac": achieved_tflops / peak,
-                                        "peak_source": f"{props.multi_processor_count} SMs x 128 lanes x 2 "
-                                                       f"at the measured {mhz:.0f} MHz"})
     # the plain one-system-per-launch path on the same GPU (rank 0, N = 1)
     if rank == 0 and ws == 1 and not args.no_plain:
         pv, psample = plain_sample(engine, specs, checked, args.plain_replicas)
@@ -608,9 +644,10 @@ def run_engine(args):
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         from oracle import bind
         if bind.have_reference():
-            v, sample = cpu_sample(specs, threads, args.cpu_budget)
-            out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
-                                   "sample": sample}
+            pick, stride = sample_indices(len(specs), threads)
+            v, sample = cpu_samples([specs[i] for i in pick], len(specs), stride, threads, args.cpu_budget)
+            out["cpu_baseline"] = {"value": v[0] if v else None, "unit": UNIT, "cores": threads,
+                                   "kind": "reference", "sample": sample}
         else:
             out["cpu_baseline"] = None
     if rank == 0:
@@ -630,7 +667,7 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--replicas", type=int, default=256)
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of the CPU-baseline sample")
-    ap.add_argument("--ref-budget", type=float, default=10.0, help="seconds per reference-arm step")
+    ap.add_argument("--ref-budget", type=float, default=3.0, help="seconds per reference-arm step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the one-system-per-launch measurement")
     ap.add_argument("--plain-replicas", type=int, default=16)

@@ -178,15 +178,29 @@ def chain(n_atoms: int, charge: float, rng: np.random.Generator) -> Species:
     0-2 kcal/mol) carrying hydrogens at 1.0-1.09 A; heavy-atom charges
     N(0, 0.3 e) shifted to the net charge, hydrogen charges |N(0.1, 0.04)| e
     (small and positive, so that no H-H pair attracts through the soft H core);
-    LJ sigma 2.5-3.5 A, eps 0.02-0.2 (H: 2.5 A, 0.03).  Hydrogens are turned
-    about their heavy atom for the largest clearance, and a geometry is kept
-    only if every pair outside the AMBER exclusions (1-2, 1-3, 1-4) is at
-    least 0.7 sigma apart."""
+    LJ sigma 2.5-3.5 A, eps 0.02-0.2 (H: 2.5 A, 0.03).  Heavy atoms are
+    tetravalent: two hydrogens on each interior atom, up to three on each
+    end, placed at tetrahedral angles (the ends' cones turned for the largest
+    clearance), so that no H-X-X equilibrium angle nears 180 deg, where the
+    torsions through the hydrogen are singular.  A geometry is kept only if
+    every pair outside the AMBER exclusions (1-2, 1-3, 1-4) is at least
+    0.7 sigma apart."""
     n_heavy = max(3, n_atoms // 3)
     n_h = n_atoms - n_heavy
     n_heavy_types = 6
-    per = np.full(n_heavy, n_h // n_heavy)
-    per[: n_h % n_heavy] += 1
+    # tetravalent heavy atoms: two hydrogens on each interior atom, the
+    # remainder (at most three each) on the two chain ends
+    if n_h > 2 * n_heavy + 2:
+        raise ValueError(f"{n_atoms} atoms need more hydrogens than {n_heavy} heavy atoms carry")
+    per = np.zeros(n_heavy, np.int64)
+    left = n_h
+    for i in [0, n_heavy - 1] + list(range(1, n_heavy - 1)):
+        per[i] = min(left, 2)
+        left -= per[i]
+    for i in (0, n_heavy - 1):
+        take = min(left, 1)
+        per[i] += take
+        left -= take
     hpar = [i for i in range(n_heavy) for _ in range(per[i])]
     mass = list(rng.choice([12.011, 14.007, 15.999], n_heavy_types)) + [1.008]
     eps = list(rng.uniform(0.02, 0.2, n_heavy_types)) + [0.03]
@@ -274,26 +288,41 @@ def chain(n_atoms: int, charge: float, rng: np.random.Generator) -> Species:
                 continue
             nb = [j for j in (i - 1, i + 1) if 0 <= j < n_heavy]
             u = -sum((bb[j] - bb[i]) / np.linalg.norm(bb[j] - bb[i]) for j in nb)
-            if np.linalg.norm(u) < 1e-3:
-                u = _perp(bb[nb[0]] - bb[i], rng)
             u /= np.linalg.norm(u)
-            w0 = _perp(u, rng)
-            best, best_pos = -1.0, None
-            for k in range(24):
-                phi = 2 * math.pi * k / 24
-                w = w0 * math.cos(phi) + np.cross(u, w0) * math.sin(phi)
-                pos = []
-                for hidx, hh in enumerate(hs_of[i]):
-                    ang = phi + 2 * math.pi * hidx / len(hs_of[i])
-                    v = w0 * math.cos(ang) + np.cross(u, w0) * math.sin(ang)
-                    dirn = math.cos(54.75 * DEG) * u + math.sin(54.75 * DEG) * v
-                    pos.append(bb[i] + 1.045 * dirn)
-                pos = np.array(pos)
-                others = np.concatenate([bb[[j for j in range(n_heavy) if abs(j - i) > 1]],
-                                         xs[n_heavy:][[h for h in range(n_h) if hpar[h] < i]]])
-                m = np.linalg.norm(pos[:, None] - others[None], axis=2).min() if len(others) else 9.0
-                if m > best:
-                    best, best_pos = m, pos
+            nh = len(hs_of[i])
+            others = np.concatenate([bb[[j for j in range(n_heavy) if abs(j - i) > 1]],
+                                     xs[n_heavy:][[h for h in range(n_h) if hpar[h] < i]]])
+            if len(nb) == 2:
+                # interior atom: the hydrogens in the plane through the
+                # bisector u normal to the backbone plane, 109.5 deg apart
+                # (one hydrogen: along u), so every H-X-X angle is near
+                # tetrahedral and none approaches 180 deg, where the torsions
+                # through the hydrogen become singular
+                n_pl = np.cross(bb[nb[0]] - bb[i], bb[nb[1]] - bb[i])
+                n_pl /= np.linalg.norm(n_pl)
+                if nh == 1:
+                    dirs = [u]
+                else:
+                    a = 0.5 * 109.47 * DEG
+                    dirs = [math.cos(a) * u + math.sin(a) * n_pl, math.cos(a) * u - math.sin(a) * n_pl]
+                best_pos = np.array([bb[i] + 1.045 * d for d in dirs])
+            else:
+                # chain end: a cone at 109.5 deg from the one backbone bond,
+                # turned about it for the largest clearance
+                w0 = _perp(u, rng)
+                best, best_pos = -1.0, None
+                for k in range(24):
+                    phi = 2 * math.pi * k / 24
+                    pos = []
+                    for hidx in range(nh):
+                        ang = phi + 2 * math.pi * hidx / 3  # tetrahedral sites
+                        v = w0 * math.cos(ang) + np.cross(u, w0) * math.sin(ang)
+                        dirn = math.cos(70.53 * DEG) * u + math.sin(70.53 * DEG) * v
+                        pos.append(bb[i] + 1.045 * dirn)
+                    pos = np.array(pos)
+                    m = np.linalg.norm(pos[:, None] - others[None], axis=2).min() if len(others) else 9.0
+                    if m > best:
+                        best, best_pos = m, pos
             for hidx, hh in enumerate(hs_of[i]):
                 xs[hh] = best_pos[hidx]
         for h in range(n_h):  # bond lengths 1.0-1.09 A
