@@ -1052,6 +1052,7 @@ __device__ void gas_far_pass_t(Ctx& x, bool eflag, bool kick) {
   constexpr int ag = AG;
   const int par = x.D->parity;
   const bool intra = term_on(x, MDN_I_GAS_INTRA) && P->n_gas_bonds > 0;
+  const bool gg = term_on(x, MDN_I_GG) && P->ggl_cap > 0;
   int lo, hi;
   partition(x, x.D->n_gas_in, &lo, &hi);
   double c2[AG];
@@ -1072,6 +1073,9 @@ __device__ void gas_far_pass_t(Ctx& x, bool eflag, bool kick) {
       double e = gas_intra<AG>(x, X, F);
       if (eflag) eg += efixd(e);
     }
+    if (gg)
+      for (int at = 0; at < ag; at++)
+        for (int k = 0; k < 3; k++) F[3 * at + k] += a->slab_fgg[3 * gatom(P, par, s, at) + k];
     for (int at = 0; at < ag; at++) {
       size_t g = gatom(P, par, s, at);
       for (int k = 0; k < 3; k++) {
@@ -1091,6 +1095,108 @@ __device__ void gas_far_pass(Ctx& x, bool eflag, bool kick) {
   else gas_far_pass_t<2>(x, eflag, kick);
 }
 
+/* gas-gas LJ, the corrected form of PotentialGasGas::compute
+ * (src/potential/GasGas.cpp:4-38): every atom pair of two listed in-domain
+ * gas molecules, force x w_i w_j with both atoms' taper weights, energy
+ * unweighted into Ugg.  The reference's own routine pairs loop indices
+ * instead of gas_in entries (:48-57), reads weight[0][jj] (:25), bounds the
+ * partner loop by the first molecule's size (:13) and books the energy in
+ * Uvg (:34); none of that is reproduced.  One thread per slab molecule of
+ * this CTA walks its full (both-direction) partner list and writes its own
+ * force, so no reaction is scattered and the sum does not depend on the
+ * launch shape.  Weights come from the current positions and ion centre, as
+ * MD::update_position sets them (src/verlet.cpp:109-134); molecules the
+ * rebuild of this step inserted have weight 0 (`fresh`: this step rebuilt). */
+template <int AG, bool FP64>
+__device__ __noinline__ void gas_gg_pass_t(Ctx& x, bool eflag, bool fresh) {
+  const RepParams* P = x.P;
+  const KArgs* a = x.a;
+  const int par = x.D->parity, nt = P->n_types, nreb = x.D->n_rebuilds;
+  int lo, hi;
+  partition(x, x.D->n_gas_in, &lo, &hi);
+  int gtype[AG];
+#pragma unroll
+  for (int at = 0; at < AG; at++) gtype[at] = x.ib[P->o_gas_type + at];
+  const double* com = x.D->ion_com;
+  long long egg = 0;
+  for (int s = lo + (int)threadIdx.x; s < hi; s += blockDim.x) {
+    const size_t ms = gmol(P, par, s);
+    const bool s_new = fresh && a->slab_ins[ms] == nreb;
+    double X[3 * AG], w[AG];
+    float3 gp[AG];
+#pragma unroll
+    for (int at = 0; at < AG; at++) {
+      const size_t g = gatom(P, par, s, at);
+      for (int k = 0; k < 3; k++) X[3 * at + k] = a->slab_x[3 * g + k];
+      gp[at] = make_float3((float)(X[3 * at] - com[0]), (float)(X[3 * at + 1] - com[1]),
+                           (float)(X[3 * at + 2] - com[2]));
+      w[at] = s_new ? 0.0 : taper(P, com, X + 3 * at);
+    }
+    long long F[AG][3];
+#pragma unroll
+    for (int at = 0; at < AG; at++) F[at][0] = F[at][1] = F[at][2] = 0;
+    const int start = a->ggl_start[ms], cnt = a->ggl_n[ms];
+    for (int q = 0; q < cnt; q++) {
+      const int t = a->ggl[P->ggl_off + start + q];
+      const bool t_new = fresh && a->slab_ins[gmol(P, par, t)] == nreb;
+#pragma unroll
+      for (int b = 0; b < AG; b++) {
+        const size_t gt = gatom(P, par, t, b);
+        const double Y[3] = {a->slab_x[3 * gt], a->slab_x[3 * gt + 1], a->slab_x[3 * gt + 2]};
+        const double wb = t_new ? 0.0 : taper(P, com, Y);
+        const int tb = gtype[b];
+#pragma unroll
+        for (int at = 0; at < AG; at++) {
+          const int ta = gtype[at];
+          long long fx, fy, fz;
+          if constexpr (FP64) {
+            const double ex = X[3 * at] - Y[0], ey = X[3 * at + 1] - Y[1], ez = X[3 * at + 2] - Y[2];
+            const double fd = lj_coul_d(ex * ex + ey * ey + ez * ez, x.db[P->d_ljA + ta * nt + tb],
+                                        x.db[P->d_ljB + ta * nt + tb], 0.0, false) * (w[at] * wb);
+            fx = fixd(fd * ex); fy = fixd(fd * ey); fz = fixd(fd * ez);
+          } else {
+            const float dx = gp[at].x - (float)(Y[0] - com[0]), dy = gp[at].y - (float)(Y[1] - com[1]),
+                        dz = gp[at].z - (float)(Y[2] - com[2]);
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            float ee;
+            const float fp = lj_coul(r2, x.c.ljA[ta * nt + tb], x.c.ljB[ta * nt + tb], 0.0f, false, &ee) *
+                             (float)(w[at] * wb);
+            fx = fixf(fp * dx); fy = fixf(fp * dy); fz = fixf(fp * dz);
+          }
+          F[at][0] += fx; F[at][1] += fy; F[at][2] += fz;
+          if (eflag && t > s)
+            egg += efixd(lj_coul_energy(r2d(X + 3 * at, Y), x.db[P->d_ljA + ta * nt + tb],
+                                        x.db[P->d_ljB + ta * nt + tb], 0.0));
+        }
+      }
+    }
+#pragma unroll
+    for (int at = 0; at < AG; at++) {
+      const size_t g = gatom(P, par, s, at);
+      for (int k = 0; k < 3; k++) {
+        const double f = (double)F[at][k] * MDN_FIX_INV;
+        if (!(fabs(f) < MDN_FIX_LIMIT)) set_status(x, MDN_ST_FIXED_OVERFLOW);
+        a->slab_fgg[3 * g + k] = f;
+      }
+    }
+  }
+  if (eflag) {
+    egg = warp_sum_ll(egg);
+    if ((threadIdx.x & 31) == 0) energy_add(x, MDN_U_GG, egg);
+  }
+}
+
+/* the gas-gas forces of this step, when gg LJ is on: every CTA of the
+ * cluster must see the final gas positions first */
+__device__ void gas_gg_pass(Ctx& x, cg::cluster_group& cl, bool eflag, bool fresh) {
+  if (!(term_on(x, MDN_I_GG) && x.P->ggl_cap > 0)) return;
+  __threadfence();
+  cl.sync();
+  if (x.P->a_g == 1) gas_gg_pass_t<1, kFP64Pairs>(x, eflag, fresh);
+  else gas_gg_pass_t<2, kFP64Pairs>(x, eflag, fresh);
+  __syncthreads();
+}
+
 /* near molecules (those with a gas-ion or gas-vapor list entry): one thread
  * each, walking the molecule's lists (about one entry per molecule in the
  * batched workload, so a wider split leaves lanes idle); the molecule's own
@@ -1105,6 +1211,7 @@ __device__ void gas_near_pass_t(Ctx& x, bool eflag, bool kick) {
   const int av = P->a_v, par = x.D->parity, nt = P->n_types, ni = P->n_ion;
   const bool gi = term_on(x, MDN_I_GI), gv = term_on(x, MDN_I_GV);
   const bool intra = term_on(x, MDN_I_GAS_INTRA) && P->n_gas_bonds > 0;
+  const bool gg = term_on(x, MDN_I_GG) && P->ggl_cap > 0;
   const int nj = (P->quirks & MDN_Q_GV_GAS_COUNT) ? min(ag, av) : av;
   int lo, hi;
   partition(x, x.D->n_gas_in, &lo, &hi);
@@ -1216,6 +1323,9 @@ __device__ void gas_near_pass_t(Ctx& x, bool eflag, bool kick) {
         Fd[3 * at + k] = (double)F[at][k] * MDN_FIX_INV;
         if (!(fabs(Fd[3 * at + k]) < MDN_FIX_LIMIT)) set_status(x, MDN_ST_FIXED_OVERFLOW);
       }
+    if (gg)
+      for (int at = 0; at < ag; at++)
+        for (int k = 0; k < 3; k++) Fd[3 * at + k] += a->slab_fgg[3 * gatom(P, par, s, at) + k];
     if (intra) {
       double ei = gas_intra<AG>(x, X, Fd);
       if (eflag) eintra += efixd(ei);
@@ -1484,6 +1594,64 @@ __device__ void cluster_prefix(Ctx& x, cg::cluster_group& cl, int* slot_in_smem,
   cl.sync();
 }
 
+/* gas-gas pair list of the slab (PotentialGasGas::makePair,
+ * src/potential/GasGas.cpp:41-62, on the in-domain molecules it was meant
+ * for): every other slab molecule whose centre lies within the list radius,
+ * both directions, ascending slab slot, CSR by slab slot over the cluster */
+__device__ void relist_gg(Ctx& x, cg::cluster_group& cl) {
+  const RepParams* P = x.P;
+  const KArgs* a = x.a;
+  const int par = x.D->parity, G = x.D->n_gas_in;
+  int lo, hi;
+  partition(x, G, &lo, &hi);
+  int* sc = x.iscr;
+  const double* cen = a->mol_x + 3 * ((size_t)P->mol_off + 1);
+  const int* smol = a->slab_mol + gmol(P, par, 0);
+  auto partners = [&](int s, int* out) {
+    const double* c = cen + 3 * (size_t)smol[s];
+    int n = 0;
+    for (int t = 0; t < G; t++) {
+      if (t == s) continue;
+      const double* d = cen + 3 * (size_t)smol[t];
+      const double dx = c[0] - d[0], dy = c[1] - d[1], dz = c[2] - d[2];
+      if ((dx * dx + dy * dy + dz * dz) < P->ml2) {
+        if (out) out[n] = t;
+        n++;
+      }
+    }
+    return n;
+  };
+  int mine = 0;
+  for (int s = lo + (int)threadIdx.x; s < hi; s += blockDim.x) mine += partners(s, nullptr);
+  mine = block_sum_i(mine, sc);
+  int base, tot;
+  cluster_prefix(x, cl, &sc[46], mine, &base, &tot);
+  const bool over = tot > P->ggl_cap;
+  if (over && threadIdx.x == 0 && x.rank == 0) set_status(x, MDN_ST_LIST_OVERFLOW);
+  int run = base;
+  for (int s0 = lo; s0 < hi; s0 += blockDim.x) {
+    const int s = s0 + threadIdx.x;
+    const int c = s < hi ? partners(s, nullptr) : 0;
+    int t_tot;
+    const int off = block_exscan(c, sc, &t_tot);
+    if (s < hi) {
+      const size_t ms = gmol(P, par, s);
+      if (!over) {
+        a->ggl_start[ms] = run + off;
+        a->ggl_n[ms] = c;
+        partners(s, a->ggl + P->ggl_off + run + off);
+      } else {
+        a->ggl_start[ms] = 0;
+        a->ggl_n[ms] = 0;
+      }
+    }
+    run += t_tot;
+  }
+  if (threadIdx.x == 0) x.D->gg_count = over ? 0 : tot / 2;
+  __threadfence();
+  cl.sync();
+}
+
 /* pair lists of the gas slab (current parity) from the centres: gas-ion
  * (PotentialGasIon::makePair) and gas-vapor (PotentialVaporGas::makePair) */
 __device__ void relist(Ctx& x, cg::cluster_group& cl) {
@@ -1598,6 +1766,7 @@ __device__ void relist(Ctx& x, cg::cluster_group& cl) {
   }
   __threadfence();
   cl.sync();
+  if (P->ggl_cap > 0 && (P->interactions & MDN_I_GG)) relist_gg(x, cl);
 }
 
 /* The overlap test of entering vapor molecules: against the ion, the vapor
@@ -1831,6 +2000,7 @@ __device__ void make_pair(Ctx& x, cg::cluster_group& cl) {
           }
         }
         a->slab_mol[gmol(P, npar, ns)] = q;
+        if (a->slab_ins) a->slab_ins[gmol(P, npar, ns)] = (f & 2) ? -1 : nreb + 1;
         a->slot[g] = ns;
       } else {
         a->slot[g] = -1;
@@ -1922,7 +2092,10 @@ __device__ void one_step(Ctx& x, cg::cluster_group& cl, bool eflag) {
     __syncthreads();
   }
   const bool rebuild = x.D->loop_pair + 1 > x.D->loop_update;
-  core_drift_shake(x, !rebuild, eflag);
+  /* with gas-gas forces no gas molecule can take its force during its own
+   * drift: they need every molecule's new position */
+  const bool gg = (P->interactions & MDN_I_GG) && P->ggl_cap > 0;
+  core_drift_shake(x, !rebuild && !gg, eflag);
   ion_centre(x);
   if (x.D->nvt_mode == MDN_NVT_NH) {
     double T = ion_temperature(x);
@@ -1941,6 +2114,11 @@ __device__ void one_step(Ctx& x, cg::cluster_group& cl, bool eflag) {
   if (rebuild) {
     prof_start(x);
     make_pair(x, cl);
+    prof_end(x, MDN_PROF_REBUILD);
+  }
+  if (gg) gas_gg_pass(x, cl, eflag, rebuild);
+  if (rebuild || gg) {
+    prof_start(x);
     gas_far_pass(x, eflag, true);
     __syncthreads();
     prof_end(x, MDN_PROF_REBUILD);
@@ -2056,6 +2234,7 @@ extern "C" __global__ void __launch_bounds__(512, 1) MDN_ADVANCE_KERNEL(KArgs a)
       __syncthreads();
       ion_centre(x);
       core_weights_pos(x, false);
+      gas_gg_pass(x, cl, true, false);
       gas_far_pass(x, true, false);
       __syncthreads();
       forces_and_kick(x, cl, true, false);

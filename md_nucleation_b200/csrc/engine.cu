@@ -123,6 +123,8 @@ struct mdn_handle {
   int* near_list = nullptr;
   int *near_gi = nullptr, *near_gv = nullptr;
   unsigned short *gil_n = nullptr, *gvl_n = nullptr, *gil = nullptr, *gvl = nullptr;
+  int *ggl_start = nullptr, *ggl_n = nullptr, *ggl = nullptr, *slab_ins = nullptr;
+  double* slab_fgg = nullptr;
   long long* energy = nullptr;
   DevEvent* events = nullptr;
   int* n_events = nullptr;
@@ -148,7 +150,7 @@ struct mdn_handle {
   bool prof_on = false;
   /* sizes */
   size_t n_ion_tot = 0, n_mol_tot = 0, n_slab_atoms = 0, n_slab_mols = 0, n_vslab_atoms = 0,
-         n_vslab_mols = 0, n_near = 0, n_gil = 0, n_gvl = 0;
+         n_vslab_mols = 0, n_near = 0, n_gil = 0, n_gvl = 0, n_ggl = 0;
   double last_ms = 0;
   long long last_launches = 0;
   /* snapshot staging */
@@ -167,7 +169,8 @@ void free_all(mdn_handle* h) {
                   h->vslab_f, h->vslab_w, h->vslab_mol, h->near_list, h->near_gi, h->near_gv, h->gil_n,
                   h->gvl_n, h->gil, h->gvl, h->energy, h->events, h->n_events, h->status, h->job_order,
                   h->job_counter, h->snap_off, h->snap_type, h->snap_x, h->snap_v, h->d_ctl_mode,
-                  h->d_ctl_T, h->d_prof, h->job_order2, h->job_counter2};
+                  h->d_ctl_T, h->d_prof, h->job_order2, h->job_counter2, h->ggl_start, h->ggl_n, h->ggl,
+                  h->slab_fgg, h->slab_ins};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -263,6 +266,8 @@ long long launch(mdn_handle* h, int mode, long long n_steps, int energy_mode, un
   a.vslab_mol = h->vslab_mol;
   a.near_list = h->near_list; a.near_gi = h->near_gi; a.near_gv = h->near_gv;
   a.gil_n = h->gil_n; a.gvl_n = h->gvl_n; a.gil = h->gil; a.gvl = h->gvl;
+  a.ggl_start = h->ggl_start; a.ggl_n = h->ggl_n; a.ggl = h->ggl;
+  a.slab_fgg = h->slab_fgg; a.slab_ins = h->slab_ins;
   a.energy = h->energy;
   a.events = h->events; a.n_events = h->n_events; a.ev_cap = h->ev_cap;
   a.status = h->status;
@@ -389,7 +394,7 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
   h->P.resize(R);
   h->D0.resize(R);
   size_t ion_tot = 0, mol_tot = 0, slab_atoms = 0, slab_mols = 0, vslab_atoms = 0, vslab_mols = 0, near_tot = 0,
-         gil_tot = 0, gvl_tot = 0;
+         gil_tot = 0, gvl_tot = 0, ggl_tot = 0;
   for (int r = 0; r < R; r++) {
     const mdn_replica_desc& d = descs[r];
     RepParams& P = h->P[r];
@@ -399,7 +404,6 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
     if (d.gas.n_atoms < 1 || d.gas.n_atoms > MDN_MAX_GAS_ATOMS) { delete h; return fail(MDN_ERR_CAPACITY, "replica %d: gas molecule of %d atoms (1..%d)", r, d.gas.n_atoms, MDN_MAX_GAS_ATOMS); }
     if (d.n_vapor > 0 && (d.vapor.n_atoms < 1 || d.vapor.n_atoms > MDN_MAX_VAP_ATOMS)) { delete h; return fail(MDN_ERR_CAPACITY, "replica %d: vapor molecule of %d atoms (1..%d)", r, d.vapor.n_atoms, MDN_MAX_VAP_ATOMS); }
     if (d.ion.n_atoms < 1 || d.ion.n_atoms > 65535) { delete h; return fail(MDN_ERR_CAPACITY, "replica %d: ion of %d atoms", r, d.ion.n_atoms); }
-    if (d.interactions & MDN_I_GG) { delete h; return fail(MDN_ERR_ARG, "replica %d: gg LJ is not available in this engine build", r); }
     if (!(d.dt > 0) || !(d.box > 0) || !(d.temperature > 0)) { delete h; return fail(MDN_ERR_ARG, "replica %d: dt, box and temperature must be positive", r); }
     int rc;
     if ((rc = check_topology(d.ion, nt, d.n_bond_types, d.n_angle_types, d.n_dihedral_types, "ion")) ||
@@ -599,6 +603,14 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
     P.gvl_cap = (int)std::min<double>((double)P.slab_cap * P.vcap, gv_est * f * 2 + 64 * P.vcap + 256);
     P.gil_cap = std::max(P.gil_cap, 16);
     P.gvl_cap = std::max(P.gvl_cap, 16);
+    /* gas-gas (both directions): partners within the list radius at the
+     * in-domain density, 1.5 x plus a margin per molecule */
+    P.ggl_cap = 0;
+    if (d.interactions & MDN_I_GG) {
+      const double partners = eg / V_sphere * 4.0 / 3.0 * M_PI * pow(rlist, 3);
+      const double est = (double)P.slab_cap * (partners * f * 1.5 + 6 * sqrt(partners) + 16);
+      P.ggl_cap = (int)std::max(16.0, std::min(std::min((double)P.slab_cap * P.slab_cap, est), 2.0e9));
+    }
 
     /* ---- pool offsets ---- */
     P.ion_off = (long long)ion_tot;
@@ -619,6 +631,8 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
     gil_tot += P.gil_cap;
     P.gvl_off = (long long)gvl_tot;
     gvl_tot += P.gvl_cap;
+    P.ggl_off = (long long)ggl_tot;
+    ggl_tot += P.ggl_cap;
     P.work = eg * P.a_g + 0.05 * pow(d.ion.n_atoms + P.vcap * P.a_v * 0.5, 2) + near_est * d.ion.n_atoms;
 
     h->nt_cap = std::max(h->nt_cap, nt);
@@ -653,6 +667,7 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
   h->n_near = near_tot;
   h->n_gil = gil_tot;
   h->n_gvl = gvl_tot;
+  h->n_ggl = ggl_tot;
 
   /* job order: largest estimated work first */
   h->order.resize(R);
@@ -709,6 +724,13 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
   ALLOC(h->gvl_n, slab_mols);
   ALLOC(h->gil, gil_tot);
   ALLOC(h->gvl, gvl_tot);
+  if (ggl_tot > 0) {
+    ALLOC(h->ggl_start, slab_mols);
+    ALLOC(h->ggl_n, slab_mols);
+    ALLOC(h->ggl, ggl_tot);
+    ALLOC(h->slab_fgg, 3 * slab_atoms);
+    ALLOC(h->slab_ins, slab_mols);
+  }
   ALLOC(h->energy, 8 * (size_t)R);
   ALLOC(h->events, (size_t)h->ev_cap);
   ALLOC(h->n_events, 1);
@@ -749,6 +771,8 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
   ck(cudaMemset(h->n_events, 0, sizeof(int)), "events");
   ck(cudaMemset(h->status, 0, sizeof(int) * R), "status");
   ck(cudaMemset(h->near_gi, 0xff, sizeof(int) * slab_mols), "near_gi");
+  if (h->slab_ins) ck(cudaMemset(h->slab_ins, 0xff, sizeof(int) * slab_mols), "slab_ins");
+  if (h->ggl_n) ck(cudaMemset(h->ggl_n, 0, sizeof(int) * slab_mols), "ggl_n");
   h->ctl_mode.resize(R);
   h->ctl_T.resize(R);
   for (int r = 0; r < R; r++) {
@@ -978,7 +1002,7 @@ int mdn_replica_info_get(mdn_handle* h, int r, mdn_replica_info* info) {
   info->status = st;
   info->gi_pairs = D.gi_count;
   info->gv_pairs = D.gv_count;
-  info->gg_pairs = 0;
+  info->gg_pairs = D.gg_count;
   return MDN_OK;
 }
 
@@ -1097,6 +1121,7 @@ int mdn_upload_state(mdn_handle* h, int r, const mdn_state* s) {
       CK(cudaMemcpy(h->slab_x + 3 * a0, x.data(), 8 * x.size(), cudaMemcpyHostToDevice));
       CK(cudaMemcpy(h->slab_v + 3 * a0, v.data(), 8 * v.size(), cudaMemcpyHostToDevice));
       CK(cudaMemcpy(h->slab_f + 3 * a0, f.data(), 8 * f.size(), cudaMemcpyHostToDevice));
+      if (h->slab_ins) CK(cudaMemset(h->slab_ins + P.slab_moff, 0xff, sizeof(int) * G));
     }
     D.n_gas_in = G;
   }
@@ -1147,10 +1172,38 @@ int mdn_upload_state(mdn_handle* h, int r, const mdn_state* s) {
 
 int mdn_pair_list(mdn_handle* h, int r, int kind, int* pairs, int capacity, int* count) {
   if (!h || r < 0 || r >= h->R || !count) return fail(MDN_ERR_ARG, "bad arguments");
-  if (kind == 2) { *count = 0; return MDN_OK; }
   const RepParams& P = h->P[r];
   RepDyn D;
   CK(cudaMemcpy(&D, h->dD + r, sizeof D, cudaMemcpyDeviceToHost));
+  if (kind == 2) {
+    /* gas-gas: (molecule, partner molecule) once per unordered pair, the
+     * lower slab slot first (ascending molecule indices, as gas_in) */
+    int c = 0;
+    const int G = D.n_gas_in, par = D.parity;
+    if (P.ggl_cap > 0 && G > 0) {
+      const size_t m0 = P.slab_moff + (size_t)par * P.slab_cap;
+      std::vector<int> mol(G), st(G), n(G);
+      CK(cudaMemcpy(mol.data(), h->slab_mol + m0, sizeof(int) * G, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(st.data(), h->ggl_start + m0, sizeof(int) * G, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(n.data(), h->ggl_n + m0, sizeof(int) * G, cudaMemcpyDeviceToHost));
+      long long tot = 0;
+      for (int i = 0; i < G; i++) tot = std::max<long long>(tot, (long long)st[i] + n[i]);
+      std::vector<int> ent(std::max<long long>(tot, 1));
+      if (tot > 0) CK(cudaMemcpy(ent.data(), h->ggl + P.ggl_off, sizeof(int) * tot, cudaMemcpyDeviceToHost));
+      for (int s_ = 0; s_ < G; s_++)
+        for (int q = 0; q < n[s_]; q++) {
+          const int t = ent[st[s_] + q];
+          if (t <= s_) continue;
+          if (c < capacity && pairs) {
+            pairs[2 * c] = mol[s_];
+            pairs[2 * c + 1] = mol[t];
+          }
+          c++;
+        }
+    }
+    *count = c;
+    return MDN_OK;
+  }
   const int G = D.n_gas_in, par = D.parity;
   std::vector<int> mol(G), st(G), vm(D.n_vap_in);
   std::vector<unsigned short> n(G);

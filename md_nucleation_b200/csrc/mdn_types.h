@@ -74,7 +74,7 @@ typedef struct RepParams {
   int d_bond, d_angle, d_dih, d_ljA, d_ljB, d_mass, d_c2;
   int d_ion_q, d_gas_x, d_gas_q, d_vap_x, d_vap_q;
   int d_ion_cons, d_gas_cons, d_vap_cons; /* per SHAKE constraint: d^2, 1/m_i, 1/m_j */
-  int pad0;
+  int ggl_cap;                   /* gas-gas list entries (both directions), 0 without gg */
   /* run parameters */
   double dt, box, ml2, ri2, RI2, rcenter, overlap, margin;
   double coeff;                  /* 0.5*dt*4.184e-4 (src/verlet.cpp:49) */
@@ -83,7 +83,7 @@ typedef struct RepParams {
   double efield[3];
   unsigned key0, key1;
   /* pool offsets (elements) */
-  long long ion_off, mol_off, slab_off, vslab_off, near_off, gil_off, gvl_off;
+  long long ion_off, mol_off, slab_off, vslab_off, near_off, gil_off, gvl_off, ggl_off;
   long long slab_moff, vslab_moff; /* molecule offsets of the two slabs */
   long long iblob_off, dblob_off;
   double work;                   /* cost estimate for the job order */
@@ -92,7 +92,7 @@ typedef struct RepParams {
 typedef struct RepDyn {
   int loop_pair, loop_update, n_rebuilds, n_gas_in;
   int n_vap_in, parity, status, n_near;
-  int gi_count, gv_count, nvt_mode, pad;
+  int gi_count, gv_count, nvt_mode, gg_count; /* gg_count: unordered gas-gas pairs */
   long long step;
   double zeta, margin_length, nvt_T, pad2;
   double ion_com[6];
@@ -124,6 +124,13 @@ typedef struct KArgs {
   int* near_gv;            /* [slab slot] start of its gv entries              */
   unsigned short *gil_n, *gvl_n; /* [slab slot] entry counts                   */
   unsigned short *gil, *gvl;
+  /* gas-gas (gg LJ, corrected form): for every slab molecule the slab slots
+   * of its partners in both directions, CSR by slab slot; the gas-gas force
+   * of each atom; the rebuild number that inserted the molecule (its taper
+   * weights are 0 on the step of that rebuild); all NULL without gg */
+  int *ggl_start, *ggl_n, *ggl;
+  double* slab_fgg;
+  int* slab_ins;
   long long* energy;       /* 8 per replica, fixed point                       */
   DevEvent* events;
   int* n_events;

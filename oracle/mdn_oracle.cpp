@@ -446,6 +446,10 @@ struct Oracle {
       ag[2] += mol_v[mi][2];
     }
     for (int k = 0; k < a_g; k++) gf[(size_t)m * a_g + k] = {0, 0, 0};
+    /* as for vapor (insert_vapor): MD::update_position ran before this
+     * rebuild, so the entering molecule's taper weights, which only the
+     * gas-gas term reads, are 0 on this step */
+    for (int k = 0; k < a_g; k++) gw[(size_t)m * a_g + k] = 0;
   }
 
   void insert_vapor(int m, int t = 0) {

@@ -83,10 +83,13 @@ def test_mdn_run_writes_the_reference_files(host, tmp_path):
     assert np.all(U[:2, 1:] == 0) and np.any(U[3:, 1:] != 0)
 
 
-def test_mdn_run_main_run_matches_oracle(host, oracle_libs, tmp_path):
+@pytest.mark.parametrize("terms", [pytest.param(TERMS, id="base"), pytest.param(TERMS | abi.I_GG, id="gg-LJ")])
+def test_mdn_run_main_run_matches_oracle(host, oracle_libs, tmp_path, terms):
+    """With `gg LJ` in the condition file too: the host takes the keyword
+    (src/initialization/setCondition.cpp:187-189) and the engine runs it."""
     d = str(tmp_path)
     cond = g.write_reference_inputs(os.path.join(d, "in"), g.nacl_cluster(), g.methanol(), gas="He", n_gas=2000,
-                                    n_vapor=20, total_steps=60, relax_steps=0, observe=30, interactions=TERMS)
+                                    n_vapor=20, total_steps=60, relax_steps=0, observe=30, interactions=terms)
     run_cli(host, cond, 9, 1, d)
     frames = read_dump(os.path.join(d, "in", "dump_9.dump"))
     assert len(frames) == 2
