@@ -127,3 +127,57 @@ def test_mdn_run_main_run_matches_oracle(host, oracle_libs, tmp_path, terms):
         gv = np.array([r[4:7] for r in got])
         assert np.abs(gx - x).max() <= tol_x + 5e-7, f"frame {k}"
         assert np.abs(gv - v).max() <= tol_v + 5e-7, f"frame {k}"
+
+
+@pytest.mark.parametrize("nvt", ["scale", "330"])
+def test_mdn_run_relaxation_matches_oracle(host, oracle_libs, tmp_path, nvt):
+    """RelaxSteps > 0 with NVTion scale or Nose-Hoover (src/run.cpp:22-30),
+    then the re-centring and rebuild (src/run.cpp:42-54, the reference's
+    shift quirk) and the NVE main run: every frame against the oracle driven
+    through the same sequence."""
+    d = str(tmp_path)
+    cond = g.write_reference_inputs(os.path.join(d, "in"), g.nacl_cluster(), g.methanol(), gas="He", n_gas=2000,
+                                    n_vapor=20, total_steps=60, relax_steps=60, observe=30, interactions=TERMS,
+                                    nvt=nvt)
+    run_cli(host, cond, 4, 1, d)
+    frames = read_dump(os.path.join(d, "in", "dump_4.dump"))
+    assert len(frames) == 4
+    s = host.HostSystem(cond, calc_number=4, place_device=0)
+    o = oracle_libs.OracleReplica.from_desc(s.desc_ptr())
+    dd = s.desc
+    assert dd.nvt_mode == (abi.NVT_SCALE if nvt == "scale" else abi.NVT_NH)
+    ion_t, gas_t, vap_t = (s.topology(w)["type"] for w in ("ion", "gas", "vapor"))
+    mass = np.array([dd.atom_mass[t] for t in range(dd.n_atom_types)])
+
+    def rows(st):
+        t, x, v = [ion_t], [st.ion_x], [st.ion_v]
+        for q in range(dd.n_gas):
+            if st.region[1 + q]:
+                t.append(gas_t), x.append(st.gas_ax[q]), v.append(st.gas_av[q])
+        for q in range(dd.n_vapor):
+            if st.region[1 + dd.n_gas + q]:
+                t.append(vap_t), x.append(st.vap_ax[q]), v.append(st.vap_av[q])
+        t, x, v = np.concatenate(t), np.vstack(x), np.vstack(v)
+        m = mass[ion_t]
+        c = (st.ion_x * m[:, None]).sum(0) / m.sum()
+        return t, x - c, v
+
+    def check(k, tol):
+        t, x, v = rows(o.get_state())
+        got = frames[k][1]
+        assert [r[0] for r in got] == [s.type_name(int(q)) for q in t], f"frame {k}: rows differ"
+        gx = np.array([r[1:4] for r in got])
+        gv = np.array([r[4:7] for r in got])
+        assert np.abs(gx - x).max() <= tol + 5e-7, f"frame {k}"
+        assert np.abs(gv - v).max() <= 0.1 * tol + 5e-7, f"frame {k}"
+
+    check(0, 1e-6)           # relaxation, step 0
+    o.step(30)
+    check(1, 2e-5)           # relaxation, step 30
+    o.step(30)
+    o.recenter(1)            # src/run.cpp:42-53
+    o.make_pair()            # src/run.cpp:54
+    o.set_nvt(abi.NVT_OFF)   # src/run.cpp:56
+    check(2, 5e-5)           # main run, step 0
+    o.step(30)
+    check(3, 1e-4)           # main run, step 30
