@@ -381,6 +381,154 @@ def placement_measurement(engine):
     return out
 
 
+def _in_domain_energy(e, r, mass):
+    """K + U of replica r's in-domain atoms after a step with energies:
+    K = sum 1/2 m v^2 (kcal/mol, the reference's real_to_kcalmol), U the sum
+    of the eight energy buckets."""
+    from md_nucleation_b200.system import REAL_TO_KCALMOL
+    t, _, v = e.in_domain(r)
+    K = 0.5 * float((mass[t] * (v * v).sum(axis=1)).sum()) * REAL_TO_KCALMOL
+    return K + float(e.energies()[r].sum()), len(t)
+
+
+def nve_drift(engine, spec, force_mode, steps, every=100):
+    """Total energy of the in-domain atoms over `steps` NVE steps with the
+    membership fixed (no rebuild in the window: loop_update set beyond it,
+    so the molecules in the domain at the start are the system, and nothing
+    enters or is resampled); the drift is the slope of a straight-line fit,
+    per ns.  The taper weights act on vapor forces but not on the energy (the
+    reference's PotentialVaporIon / PotentialVaporVapor), so a molecule in the
+    100-110 A shell moves the energy too; that is part of what is measured."""
+    from md_nucleation_b200 import abi
+    checked = abi.Q_ALL & ~abi.Q_BLIND_INSERT
+    mass = np.asarray(spec.atom_mass)
+    with engine.Engine([spec], quirks=checked, force_mode=force_mode) as e:
+        st = e.state(0)
+        st.loop_pair, st.loop_update = 0, 10 ** 8
+        e.upload(0, st)
+        t, E = [], []
+        n_atoms = 0
+        for k in range(steps // every):
+            e.step(every, energy_mode=1)
+            en, n_atoms = _in_domain_energy(e, 0, mass)
+            t.append((k + 1) * every * spec.dt)
+            E.append(en)
+        ok = e.status()[0] == 0
+    E = np.array(E)
+    slope = np.polyfit(np.array(t), E, 1)[0] * 1e6  # kcal/mol per ns
+    return {"drift_kcal_mol_per_ns": slope, "drift_per_atom_kcal_mol_per_ns": slope / max(n_atoms, 1),
+            "E_mean_kcal_mol": float(E.mean()), "E_rms_fluctuation_kcal_mol": float(E.std()),
+            "in_domain_atoms": n_atoms, "window_ps": steps * spec.dt / 1000, "status_clean": bool(ok)}
+
+
+def force_energy_error(engine, specs, steps=20):
+    """FP32 pair terms (force_mode 0) against FP64 pair terms (force_mode 1,
+    which the parity tests hold within 1e-9 of the FP64 oracle) on the same
+    states: relative RMS of the in-domain forces, and the largest energy
+    bucket difference relative to the largest bucket, per replica."""
+    from md_nucleation_b200 import abi
+    checked = abi.Q_ALL & ~abi.Q_BLIND_INSERT
+    out = []
+    with engine.Engine(specs, quirks=checked, force_mode=1) as e64, \
+            engine.Engine(specs, quirks=checked, force_mode=0) as e32:
+        e64.step(steps)
+        for r, sp in enumerate(specs):
+            st = e64.state(r)
+            e32.upload(r, st)
+            e64.upload(r, st)
+        e64.compute_forces(0)
+        e32.compute_forces(0)
+        U64, U32 = e64.energies(), e32.energies()
+        for r, sp in enumerate(specs):
+            a, b = e32.state(r), e64.state(r)
+            g = b.region[1:1 + sp.n_gas].astype(bool)
+            v = b.region[1 + sp.n_gas:].astype(bool)
+            fa = np.concatenate([a.ion_f.reshape(-1, 3), a.gas_af[g].reshape(-1, 3), a.vap_af[v].reshape(-1, 3)])
+            fb = np.concatenate([b.ion_f.reshape(-1, 3), b.gas_af[g].reshape(-1, 3), b.vap_af[v].reshape(-1, 3)])
+            ferr = float(np.sqrt(((fa - fb) ** 2).sum() / max((fb ** 2).sum(), 1e-300)))
+            scale = max(float(np.abs(U64[r]).max()), 1e-12)
+            out.append({"force_rel_rms": ferr,
+                        "energy_rel": float(np.abs(U32[r] - U64[r]).max()) / scale,
+                        "U_total_fp64": float(U64[r].sum()), "U_total_fp32": float(U32[r].sum())})
+    return out
+
+
+C4_GAS, C4_VAPOR = 1_000_000, 1000
+
+
+def _config4_unplaced(r):
+    """A configuration-4 replica without its molecules (the bench places
+    them with mdn_place on the GPU; nothing to pickle back from the pool)"""
+    from md_nucleation_b200 import generate
+
+    def later(box, ion_x, n_gas, n_vap, gs, vs, seed):
+        e = np.zeros((0, 3))
+        return e, e, e, e
+    return generate.config4_replica(r, n_gas=C4_GAS, n_vap=C4_VAPOR, placer=later)
+
+
+def config4_specs(engine, n, workers):
+    """n configuration-4 replicas (1,000,000 N2, 1,000 rigid water at 10 Pa,
+    the 500-atom +2 chain): chains grown in a spawn pool, molecules placed
+    by mdn_place (the reference's placement rule, on the GPU)."""
+    from md_nucleation_b200.system import mb_sigma
+    with mp.get_context("spawn").Pool(max(1, min(workers, n))) as pool:
+        specs = pool.map(_config4_unplaced, range(n), chunksize=1)
+    for sp in specs:
+        gx, gv, vx, vv = engine.place(sp.box, sp.ion.x, C4_GAS, C4_VAPOR,
+                                      mb_sigma(sp.temperature, sp.gas_mb_mass),
+                                      mb_sigma(sp.temperature, sp.vapor_mb_mass), sp.seed)
+        sp.gas_x, sp.gas_v, sp.vapor_x, sp.vapor_v = gx, gv, vx, vv
+    return specs
+
+
+def accuracy_report(engine, specs2, c4specs, drift_steps):
+    """The numbers the FP32 pair arithmetic is judged by, per configuration:
+    FP32-vs-FP64 force and energy error, and the NVE energy drift per ns of
+    both pair modes in a fixed-membership window."""
+    from md_nucleation_b200 import generate
+    out = {}
+    cfg = {"config0": generate.config0(0), "config1": generate.config1(0)}
+    for name, sp in cfg.items():
+        out[name] = {"fp32_vs_fp64": force_energy_error(engine, [sp])[0],
+                     "nve_fp32": nve_drift(engine, sp, 0, drift_steps),
+                     "nve_fp64": nve_drift(engine, sp, 1, drift_steps)}
+    pick = [0, len(specs2) // 3, 2 * len(specs2) // 3, len(specs2) - 1]
+    sample = [specs2[i] for i in pick]
+    errs = force_energy_error(engine, sample)
+    out["config2"] = {"replicas": pick, "fp32_vs_fp64": errs,
+                      "nve_fp32": [nve_drift(engine, sample[k], 0, drift_steps // 2) for k in (0, 3)],
+                      "nve_fp64": [nve_drift(engine, sample[k], 1, drift_steps // 2) for k in (0, 3)]}
+    if c4specs:
+        out["config4"] = {"fp32_vs_fp64": force_energy_error(engine, c4specs[:2])}
+    return out
+
+
+def config4_measurement(engine, specs, blocks):
+    """Configuration 4 batched: 16 replicas of 1,000,000 N2, 1,000 water and
+    the 500-atom chain, advanced in 100-step launches with the checked
+    insertion; device time from CUDA events."""
+    from md_nucleation_b200 import abi
+    checked = abi.Q_ALL & ~abi.Q_BLIND_INSERT
+    with engine.Engine(specs, quirks=checked, use_graph=1) as e:
+        e.step(100)
+        i0 = [e.info(r) for r in range(e.n)]
+        ms = 0.0
+        for _ in range(blocks):
+            e.step(100)
+            ms += e.last_timing()[0]
+        i1 = [e.info(r) for r in range(e.n)]
+        st = e.status()
+    a0 = in_domain_atoms(i0, specs)
+    a1 = in_domain_atoms(i1, specs)
+    atom_steps = 0.5 * float(a0.sum() + a1.sum()) * 100 * blocks
+    return {"replicas": len(specs), "molecules_per_replica": specs[0].n_mol, "md_steps": 100 * blocks,
+            "value": atom_steps / (ms * 1e-3), "unit": UNIT, "ms_per_100_steps": ms / blocks,
+            "in_domain_atoms": int(a1.sum()), "rebuilds": int(sum(i.n_rebuilds for i in i1)),
+            "replicas_failed": int(np.sum((st & abi.ST_FATAL) != 0)),
+            "ns_per_day_per_replica": 100 * blocks * specs[0].dt * 1e-6 / (ms * 1e-3) * 86400}
+
+
 def adjoint_measurement(engine):
     """The gradient harness on the adjoint configuration: a 2,000-step window
     of the production system (150-atom +1 chain, 100 methanol, 100,000 rigid
@@ -640,6 +788,18 @@ def run_engine(args):
     # initial placement of the configuration-4 system (rank 0, N = 1)
     if rank == 0 and ws == 1 and not args.no_placement:
         out["placement"] = placement_measurement(engine)
+    # ns/day of the batched run: every replica advances MD_STEPS * dt per step
+    if rank == 0:
+        per = MD_STEPS * specs[0].dt * 1e-6 / (ms_max / args.steps * 1e-3) * 86400
+        out["ns_per_day"] = {"per_replica": per, "aggregate": per * eng.n * ws}
+    # configuration 4 batched and the accuracy report (rank 0, N = 1)
+    if rank == 0 and ws == 1 and not args.no_accuracy:
+        t0 = time.time()
+        c4 = config4_specs(engine, args.config4_replicas, threads) if args.config4_replicas else []
+        if c4:
+            out["config4"] = config4_measurement(engine, c4, args.config4_blocks)
+        out["accuracy"] = accuracy_report(engine, specs, c4, args.drift_steps)
+        log(f"config 4 and accuracy report in {time.time() - t0:.0f} s")
     # CPU baseline on rank 0 at N = 1 only
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         from oracle import bind
@@ -673,6 +833,11 @@ def main():
     ap.add_argument("--plain-replicas", type=int, default=16)
     ap.add_argument("--no-adjoint", action="store_true", help="skip the gradient-harness measurement")
     ap.add_argument("--no-placement", action="store_true", help="skip the initial-placement measurement")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip configuration 4 and the FP32/FP64 accuracy and NVE drift report")
+    ap.add_argument("--config4-replicas", type=int, default=16)
+    ap.add_argument("--config4-blocks", type=int, default=10, help="100-step launches of configuration 4")
+    ap.add_argument("--drift-steps", type=int, default=10000, help="NVE window of the drift measurement")
     ap.add_argument("--cluster", type=int, default=0, help="CTAs per replica (1..8); 0 = tuned in the warm-up")
     ap.add_argument("--threads", type=int, default=0, help="threads per CTA (multiple of 32, <= 512); 0 = 512")
     ap.add_argument("--split", type=int, default=0,

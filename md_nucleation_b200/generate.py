@@ -400,7 +400,7 @@ def assemble(ion: Species, gas: Species, vap: Species, *, gas_name: str, n_gas: 
              n_vap: int, T: float, p: float, dt: float, interactions: int, seed: int,
              shake_h: bool, rng: np.random.Generator, nvt_mode=abi.NVT_OFF,
              min_dist: float = 10.0, box: Optional[float] = None, label: str = "",
-             reference_masses: bool = False) -> ReplicaSpec:
+             reference_masses: bool = False, placer=None) -> ReplicaSpec:
     """Concatenates the species' tables (ion, gas, vapor order), places the
     molecules uniformly in the cube and draws Maxwell-Boltzmann velocities.
 
@@ -410,7 +410,12 @@ def assemble(ion: Species, gas: Species, vap: Species, *, gas_name: str, n_gas: 
     used by src/initialization/initializationGas.cpp:61): 4.0026 for He, whose
     atom is 4.027, and 39.948 for Ar, whose atom is 28.02
     (src/initialization/setCondition.cpp:50,104); the argon centre of mass
-    then moves 30% off its atom."""
+    then moves 30% off its atom.
+
+    placer, when given, replaces the placement and the molecules' velocities:
+    placer(box, ion_x, n_gas, n_vap, gas_sigma, vapor_sigma, seed) returns
+    (gas_x, gas_v, vapor_x, vapor_v), e.g. engine.place (mdn_place on the GPU,
+    the reference's placement rule)."""
     offs_t, offs_b, offs_a, offs_d = [0], [0], [0], [0]
     mass, eps, sig, names = [], [], [], []
     bc, ac, dm, dc = [], [], [], []
@@ -440,6 +445,35 @@ def assemble(ion: Species, gas: Species, vap: Species, *, gas_name: str, n_gas: 
     ion_r = np.linalg.norm(ion_top.x, axis=1).max() if ion_top.n else 0.0
     if not np.all(np.isfinite(ion_top.x)):
         raise RuntimeError("non-finite ion coordinates")
+    g = GAS_TABLE[gas_name]
+    gas_com = g["mol_mass"] if reference_masses else float(sum(mass[t] for t in gas_top.type))
+    gas_m = mb_mass_kg(gas_com)
+    vap_com = float(sum(mass[t] for t in vap_top.type))
+    vap_m = mb_mass_kg(vap_com)
+    if placer is not None:
+        gx, gv, vx, vv = placer(box, ion_top.x, n_gas, n_vap, mb_sigma(T, gas_m), mb_sigma(T, vap_m), seed)
+    else:
+        gx, gv, vx, vv = _place(rng, box, ion_top.x, n_gas, n_vap, min_dist, mb_sigma(T, gas_m),
+                                mb_sigma(T, vap_m))
+    bmh = ion.bmh if ion.bmh is not None else np.zeros(ion_top.n, np.int32)
+    return ReplicaSpec(
+        atom_mass=mass, atom_eps=eps, atom_sigma=sig, atom_name=names,
+        bond_coeff=np.array(bc).reshape(-1, 2), angle_coeff=np.array(ac).reshape(-1, 2),
+        dihedral_multi=np.array(dm, np.int32), dihedral_coeff=np.array(dc).reshape(-1, 15),
+        ion=ion_top, ion_v=ion_v, ion_bmh_type=bmh,
+        gas=gas_top, gas_kind=g["kind"], gas_com_mass=gas_com, gas_mb_mass=gas_m,
+        vapor=vap_top, vapor_com_mass=vap_com, vapor_mb_mass=vap_m,
+        gas_x=gx, gas_v=gv, vapor_x=vx, vapor_v=vv,
+        dt=dt, temperature=T, box=box, interactions=interactions, nvt_mode=nvt_mode,
+        seed=seed, pressure=p, label=label)
+
+
+def _place(rng, box, ion_x, n_gas, n_vap, min_dist, gas_sigma, vap_sigma):
+    """Centres uniform in the cube: vapor first, each min_dist from the ion
+    atoms' bounding sphere and from the vapor already placed, then the gas
+    (min_dist from the ion and the vapor); Maxwell-Boltzmann velocities."""
+    half = box / 2
+    ion_r = np.linalg.norm(ion_x, axis=1).max() if len(ion_x) else 0.0
     vx = []
     tries = 0
     while len(vx) < n_vap:
@@ -466,24 +500,9 @@ def assemble(ion: Species, gas: Species, vap: Species, *, gas_name: str, n_gas: 
                 d = np.linalg.norm(c[b:b + 4096, None, :] - vx[None], axis=2).min(axis=1)
                 ok[b:b + 4096] &= d >= min_dist
         gx = np.concatenate([gx, c[ok]])[:n_gas]
-    g = GAS_TABLE[gas_name]
-    gas_com = g["mol_mass"] if reference_masses else float(sum(mass[t] for t in gas_top.type))
-    gas_m = mb_mass_kg(gas_com)
-    vap_com = float(sum(mass[t] for t in vap_top.type))
-    vap_m = mb_mass_kg(vap_com)
-    gv = rng.normal(size=(n_gas, 3)) * mb_sigma(T, gas_m)
-    vv = rng.normal(size=(n_vap, 3)) * mb_sigma(T, vap_m)
-    bmh = ion.bmh if ion.bmh is not None else np.zeros(ion_top.n, np.int32)
-    return ReplicaSpec(
-        atom_mass=mass, atom_eps=eps, atom_sigma=sig, atom_name=names,
-        bond_coeff=np.array(bc).reshape(-1, 2), angle_coeff=np.array(ac).reshape(-1, 2),
-        dihedral_multi=np.array(dm, np.int32), dihedral_coeff=np.array(dc).reshape(-1, 15),
-        ion=ion_top, ion_v=ion_v, ion_bmh_type=bmh,
-        gas=gas_top, gas_kind=g["kind"], gas_com_mass=gas_com, gas_mb_mass=gas_m,
-        vapor=vap_top, vapor_com_mass=vap_com, vapor_mb_mass=vap_m,
-        gas_x=gx, gas_v=gv, vapor_x=vx, vapor_v=vv,
-        dt=dt, temperature=T, box=box, interactions=interactions, nvt_mode=nvt_mode,
-        seed=seed, pressure=p, label=label)
+    gv = rng.normal(size=(n_gas, 3)) * gas_sigma
+    vv = rng.normal(size=(n_vap, 3)) * vap_sigma
+    return gx, gv, vx, vv
 
 
 def _shift(arr, width, col, off):
@@ -553,13 +572,15 @@ def config2(n_replicas: int = 256, scale: float = 1.0) -> List[ReplicaSpec]:
     return [config2_replica(r, scale) for r in range(n_replicas)]
 
 
-def config4_replica(replica: int = 0, n_gas: int = 1_000_000, n_vap: int = 1000) -> ReplicaSpec:
+def config4_replica(replica: int = 0, n_gas: int = 1_000_000, n_vap: int = 1000, placer=None) -> ReplicaSpec:
+    """placer: see assemble (the numpy placement of 1,000,000 molecules takes
+    about 100 s; mdn_place does it in milliseconds)."""
     rng = np.random.default_rng(seed_of(4, replica))
     ion = chain(500, 2.0, rng)
     return assemble(ion, gas_species("N2"), water(), gas_name="N2", n_gas=n_gas, n_vap=n_vap,
                     T=300.0, p=1e5, dt=1.0,
                     interactions=BASE_TERMS | abi.I_AMBER | abi.I_SHAKE,
-                    seed=seed_of(4, replica), shake_h=True, rng=rng, label="config4")
+                    seed=seed_of(4, replica), shake_h=True, rng=rng, label="config4", placer=placer)
 
 
 def small_system(seed: int = 7, gas: str = "N2", vapor: str = "methanol", ion: str = "nacl",
