@@ -532,13 +532,14 @@ def config4_measurement(engine, specs, blocks):
 def adjoint_measurement(engine):
     """The gradient harness on the adjoint configuration: a 2,000-step window
     of the production system (150-atom +1 chain, 100 methanol, 100,000 rigid
-    N2, SHAKE on X-H bonds, 300 K, 1e5 Pa) with checkpoints every 100 steps,
-    FP32 forward on the engine, FP64 adjoint.  The margin is raised to 40 A
-    so that the window holds no effective-domain rebuild (mdn_adjoint needs a
-    fixed molecule set)."""
+    N2, SHAKE on X-H bonds, 300 K, 1e5 Pa) with 8 of the methanol started
+    8-28 A from the chain (generate.config3; otherwise the domain holds no
+    vapor and the objective is identically zero), checkpoints every 100
+    steps, FP32 forward on the engine, FP64 adjoint.  The margin is raised to
+    40 A so that the window holds no effective-domain rebuild (mdn_adjoint
+    needs a fixed molecule set)."""
     from md_nucleation_b200 import generate
-    spec = generate.config1(0)
-    spec.margin = 40.0
+    spec = generate.config3(0)
     with engine.Engine([spec]) as e:
         e.step(10)
         info = e.info(0)
@@ -547,10 +548,14 @@ def adjoint_measurement(engine):
             return {"unavailable": f"the next rebuild is {info.loop_update - info.loop_pair} steps away"}
         J, grad, (fwd_ms, adj_ms) = e.adjoint(n_steps=window, checkpoint_every=100, count_radius=10.0,
                                               count_width=1.0)
+        rows, _ = e.adjoint_params()
         return {"cost_ratio": adj_ms / fwd_ms, "forward_ms": fwd_ms, "adjoint_ms": adj_ms, "n_params": len(grad),
                 "window_steps": window, "checkpoint_every": 100, "J": J,
+                "max_abs_dJ_dtheta": float(np.abs(grad).max()), "charge_scale_dJ": float(grad[-1]),
                 "in_domain_atoms": int(info.n_ion + info.n_gas_in * spec.gas.n + info.n_vapor_in * spec.vapor.n),
-                "system": "150-atom +1 chain, 100 methanol, 100,000 rigid N2 (margin 40 A)"}
+                "vapor_in_domain": int(info.n_vapor_in),
+                "system": "150-atom +1 chain, 100 methanol (8 started 8-28 A from the chain), 100,000 rigid N2 "
+                          "(margin 40 A)"}
 
 
 def host_threads():

@@ -15,7 +15,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libmdn.so")
-SOURCES = ["advance.cu", "advance_fp64.cu", "snapshot.cu", "snapshot_noalloc.cu", "adjoint.cu", "place.cu", "engine.cu"]
+SOURCES = ["advance.cu", "advance_fp64.cu", "advance_gg.cu", "advance_gg_fp64.cu", "snapshot.cu", "snapshot_noalloc.cu", "adjoint.cu", "place.cu", "engine.cu"]
 HOST = os.path.join(HERE, "host")
 HOST_SOURCES = ["mdn_host.cpp"]
 HOST_LIB = os.path.join(LIB_DIR, "libmdn_host.so")
@@ -45,13 +45,29 @@ def _stale():
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
+OBJ_DIR = os.path.join(HERE, "_build")
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compiles every CUDA source to an object concurrently (the step kernel
+    is compiled four times: FP32 / FP64 pair terms, with and without the
+    gas-gas term), then links lib/libmdn.so."""
     if force or _stale():
         os.makedirs(LIB_DIR, exist_ok=True)
-        cmd = [nvcc()] + NVCC_FLAGS + ["-shared", "-I", os.path.join(ROOT, "include"), "-I", CSRC]
-        cmd += [os.path.join(CSRC, s) for s in SOURCES] + ["-o", LIB + ".tmp"]
-        if verbose:
-            print(" ".join(cmd), file=sys.stderr)
+        os.makedirs(OBJ_DIR, exist_ok=True)
+        inc = ["-I", os.path.join(ROOT, "include"), "-I", CSRC]
+        procs, objs = [], []
+        for src in SOURCES:
+            obj = os.path.join(OBJ_DIR, os.path.splitext(src)[0] + ".o")
+            cmd = [nvcc()] + NVCC_FLAGS + inc + ["-c", os.path.join(CSRC, src), "-o", obj]
+            if verbose:
+                print(" ".join(cmd), file=sys.stderr)
+            procs.append((cmd, subprocess.Popen(cmd)))
+            objs.append(obj)
+        for cmd, p in procs:
+            if p.wait() != 0:
+                raise subprocess.CalledProcessError(p.returncode, cmd)
+        cmd = [nvcc()] + NVCC_FLAGS + ["-shared"] + objs + ["-o", LIB + ".tmp"]
         subprocess.run(cmd, check=True)
         os.replace(LIB + ".tmp", LIB)
     build_host(force=force, verbose=verbose)

@@ -601,7 +601,7 @@ __device__ void shake(const Sys& S, const Buf& B, double* y, const double* xr, d
         s2 += d * d;
       }
       double dr = s2 - dk * dk;
-      if (dr * dr > 1e-20) B.flag[0] = 0;
+      if (!(dr * dr <= 1e-20)) B.flag[0] = 0;
     }
     __syncthreads();
     const int conv = B.flag[0];

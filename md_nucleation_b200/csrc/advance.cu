@@ -225,6 +225,9 @@ __device__ __forceinline__ void shake_pair_c(double* Xi, double* Xj, const doubl
   Xj[0] -= r0 * gj; Xj[1] -= r1 * gj; Xj[2] -= r2 * gj;
 }
 
+/* (|s|^2 - d^2)^2 of one constraint; the sweeps stop when every residual is
+ * <= 1e-20 A^4 (src/shake.cpp:51-90), and a NaN residual counts as not
+ * converged, so a sweep that diverged runs into the cap and is reported */
 __device__ __forceinline__ double shake_res_c(const double* Xi, const double* Xj, const double* c) {
   double s0 = Xi[0] - Xj[0], s1 = Xi[1] - Xj[1], s2 = Xi[2] - Xj[2];
   double dr = s0 * s0 + s1 * s1 + s2 * s2 - c[0];
@@ -284,7 +287,7 @@ __device__ void core_drift_shake(Ctx& x, bool fused, bool eflag) {
       }
       bool ok = true;
       for (int k = lane; k < P->n_ion_rigid; k += 32)
-        if (shake_res_c(x.c.x + 3 * rig[3 * k], x.c.x + 3 * rig[3 * k + 1], x.db + P->d_ion_cons + 3 * k) > 1e-20)
+        if (!(shake_res_c(x.c.x + 3 * rig[3 * k], x.c.x + 3 * rig[3 * k + 1], x.db + P->d_ion_cons + 3 * k) <= 1e-20))
           ok = false;
       if (__all_sync(0xffffffffu, ok)) break;
       if (++sweeps >= MDN_SHAKE_MAX_SWEEPS) {
@@ -320,7 +323,7 @@ __device__ void core_drift_shake(Ctx& x, bool fused, bool eflag) {
           }
         conv = true;
         for (int k = 0; k < nr; k++)
-          if (shake_res_c(X + 3 * rig[3 * k], X + 3 * rig[3 * k + 1], ct + 3 * k) > 1e-20) conv = false;
+          if (!(shake_res_c(X + 3 * rig[3 * k], X + 3 * rig[3 * k + 1], ct + 3 * k) <= 1e-20)) conv = false;
       }
       if (!conv && x.rank == 0) set_status(x, MDN_ST_SHAKE_NOCONV);
       if (vcorr)
@@ -828,6 +831,14 @@ constexpr bool kFP64Pairs = false;
 
 __device__ void core_pairs(Ctx& x, bool eflag) { core_pairs_t<kFP64Pairs>(x, eflag); }
 
+/* MDN_GG_TERMS selects the gas-gas term: compiled into its own kernels
+ * (advance_gg.cu, advance_gg_fp64.cu), absent from the others */
+#ifdef MDN_GG_TERMS
+constexpr bool kGG = true;
+#else
+constexpr bool kGG = false;
+#endif
+
 __device__ void core_bonded(Ctx& x, bool eflag) {
   const RepParams* P = x.P;
   const bool amber = term_on(x, MDN_I_AMBER);
@@ -955,7 +966,7 @@ __device__ __forceinline__ int shake_gas2(const Ctx& x, double* X, const double*
     }
     converge = true;
     for (int k = 0; k < n; k++)
-      if (shake_res_c(X, X + 3, x.db + P->d_gas_cons + 3 * k) > 1e-20) converge = false;
+      if (!(shake_res_c(X, X + 3, x.db + P->d_gas_cons + 3 * k) <= 1e-20)) converge = false;
   }
   return converge ? 0 : MDN_ST_SHAKE_NOCONV;
 }
@@ -1052,7 +1063,7 @@ __device__ void gas_far_pass_t(Ctx& x, bool eflag, bool kick) {
   constexpr int ag = AG;
   const int par = x.D->parity;
   const bool intra = term_on(x, MDN_I_GAS_INTRA) && P->n_gas_bonds > 0;
-  const bool gg = term_on(x, MDN_I_GG) && P->ggl_cap > 0;
+  const bool gg = kGG && term_on(x, MDN_I_GG) && P->ggl_cap > 0;
   int lo, hi;
   partition(x, x.D->n_gas_in, &lo, &hi);
   double c2[AG];
@@ -1108,7 +1119,7 @@ __device__ void gas_far_pass(Ctx& x, bool eflag, bool kick) {
  * MD::update_position sets them (src/verlet.cpp:109-134); molecules the
  * rebuild of this step inserted have weight 0 (`fresh`: this step rebuilt). */
 template <int AG, bool FP64>
-__device__ __noinline__ void gas_gg_pass_t(Ctx& x, bool eflag, bool fresh) {
+__device__ void gas_gg_pass_t(Ctx& x, bool eflag, bool fresh) {
   const RepParams* P = x.P;
   const KArgs* a = x.a;
   const int par = x.D->parity, nt = P->n_types, nreb = x.D->n_rebuilds;
@@ -1123,13 +1134,10 @@ __device__ __noinline__ void gas_gg_pass_t(Ctx& x, bool eflag, bool fresh) {
     const size_t ms = gmol(P, par, s);
     const bool s_new = fresh && a->slab_ins[ms] == nreb;
     double X[3 * AG], w[AG];
-    float3 gp[AG];
 #pragma unroll
     for (int at = 0; at < AG; at++) {
       const size_t g = gatom(P, par, s, at);
       for (int k = 0; k < 3; k++) X[3 * at + k] = a->slab_x[3 * g + k];
-      gp[at] = make_float3((float)(X[3 * at] - com[0]), (float)(X[3 * at + 1] - com[1]),
-                           (float)(X[3 * at + 2] - com[2]));
       w[at] = s_new ? 0.0 : taper(P, com, X + 3 * at);
     }
     long long F[AG][3];
@@ -1155,8 +1163,11 @@ __device__ __noinline__ void gas_gg_pass_t(Ctx& x, bool eflag, bool fresh) {
                                         x.db[P->d_ljB + ta * nt + tb], 0.0, false) * (w[at] * wb);
             fx = fixd(fd * ex); fy = fixd(fd * ey); fz = fixd(fd * ez);
           } else {
-            const float dx = gp[at].x - (float)(Y[0] - com[0]), dy = gp[at].y - (float)(Y[1] - com[1]),
-                        dz = gp[at].z - (float)(Y[2] - com[2]);
+            /* the displacement from the FP64 positions: both atoms may sit
+             * 100 A from the ion centre, where FP32 coordinates would carry
+             * 1e-5 A of rounding into a 3 A separation */
+            const float dx = (float)(X[3 * at] - Y[0]), dy = (float)(X[3 * at + 1] - Y[1]),
+                        dz = (float)(X[3 * at + 2] - Y[2]);
             const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             float ee;
             const float fp = lj_coul(r2, x.c.ljA[ta * nt + tb], x.c.ljB[ta * nt + tb], 0.0f, false, &ee) *
@@ -1189,12 +1200,92 @@ __device__ __noinline__ void gas_gg_pass_t(Ctx& x, bool eflag, bool fresh) {
 /* the gas-gas forces of this step, when gg LJ is on: every CTA of the
  * cluster must see the final gas positions first */
 __device__ void gas_gg_pass(Ctx& x, cg::cluster_group& cl, bool eflag, bool fresh) {
-  if (!(term_on(x, MDN_I_GG) && x.P->ggl_cap > 0)) return;
-  __threadfence();
-  cl.sync();
-  if (x.P->a_g == 1) gas_gg_pass_t<1, kFP64Pairs>(x, eflag, fresh);
-  else gas_gg_pass_t<2, kFP64Pairs>(x, eflag, fresh);
-  __syncthreads();
+  if constexpr (kGG) {
+    if (!(term_on(x, MDN_I_GG) && x.P->ggl_cap > 0)) return;
+    __threadfence();
+    cl.sync();
+    if (x.P->a_g == 1) gas_gg_pass_t<1, kFP64Pairs>(x, eflag, fresh);
+    else gas_gg_pass_t<2, kFP64Pairs>(x, eflag, fresh);
+    __syncthreads();
+  }
+}
+
+/* LJ force of one (gas atom, core atom j) pair as 64-bit fixed point, the
+ * force on the gas atom (PotentialGasIon / PotentialVaporGas: no Coulomb,
+ * no taper weight).  The near pass adds it to the gas atom, the gather pass
+ * subtracts it from core atom j: one expression, so the two sides cancel
+ * exactly. */
+template <bool FP64>
+__device__ __forceinline__ void gas_core_pair(const Ctx& x, const double* Xa, float3 ga, int ta, int j,
+                                              long long* f) {
+  const RepParams* P = x.P;
+  const int nt = P->n_types, tj = x.c.type[j];
+  if constexpr (FP64) {
+    const double ex = Xa[0] - x.c.x[3 * j], ey = Xa[1] - x.c.x[3 * j + 1], ez = Xa[2] - x.c.x[3 * j + 2];
+    const double fd = lj_coul_d(ex * ex + ey * ey + ez * ez, x.db[P->d_ljA + ta * nt + tj],
+                                x.db[P->d_ljB + ta * nt + tj], 0.0, false);
+    f[0] = fixd(fd * ex); f[1] = fixd(fd * ey); f[2] = fixd(fd * ez);
+  } else {
+    const float4 pj = x.c.pos[j];
+    const float dx = ga.x - pj.x, dy = ga.y - pj.y, dz = ga.z - pj.z;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    float ee;
+    const float fp = lj_coul(r2, x.c.ljA[ta * nt + tj], x.c.ljB[ta * nt + tj], 0.0f, false, &ee);
+    f[0] = fixf(fp * dx); f[1] = fixf(fp * dy); f[2] = fixf(fp * dz);
+  }
+}
+
+/* The reactions of the near gas molecules on the core, gathered: one warp
+ * per row of the transposed lists (an ion atom, or a vapor molecule and each
+ * of its first nj atoms), its lanes over the row's gas molecules, the sum
+ * reduced across the warp and added to the core sums once.  The rows are
+ * spread over the cluster's warps. */
+template <int AG, bool FP64>
+__device__ void core_gather_t(Ctx& x) {
+  const RepParams* P = x.P;
+  const KArgs* a = x.a;
+  const int ni = P->n_ion, av = P->a_v, par = x.D->parity;
+  const int ne = ni + x.D->n_vap_in;
+  const bool gi = term_on(x, MDN_I_GI), gv = term_on(x, MDN_I_GV);
+  const int nj = (P->quirks & MDN_Q_GV_GAS_COUNT) ? min(AG, av) : av;
+  const int* tst = a->tr_start + P->tr_eoff;
+  const int* ent = a->tr + P->tr_off;
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  int gtype[AG];
+#pragma unroll
+  for (int at = 0; at < AG; at++) gtype[at] = x.ib[P->o_gas_type + at];
+  const double* com = x.D->ion_com;
+  for (int row = x.rank * nw + (int)(threadIdx.x >> 5); row < ne; row += x.C * nw) {
+    const bool ion_row = row < ni;
+    if (ion_row ? !gi : !gv) continue;
+    const int r0 = tst[row], rn = tst[row + 1] - r0;
+    const int nb = ion_row ? 1 : nj;
+    for (int b = 0; b < nb; b++) {
+      const int j = ion_row ? row : ni + (row - ni) * av + b;
+      long long R[3] = {0, 0, 0};
+      for (int q = lane; q < rn; q += 32) {
+        const int s = ent[r0 + q];
+#pragma unroll
+        for (int at = 0; at < AG; at++) {
+          const size_t g = gatom(P, par, s, at);
+          const double X[3] = {a->slab_x[3 * g], a->slab_x[3 * g + 1], a->slab_x[3 * g + 2]};
+          const float3 gp = make_float3((float)(X[0] - com[0]), (float)(X[1] - com[1]), (float)(X[2] - com[2]));
+          long long f[3];
+          gas_core_pair<FP64>(x, X, gp, gtype[at], j, f);
+          R[0] -= f[0]; R[1] -= f[1]; R[2] -= f[2];
+        }
+      }
+      R[0] = warp_sum_ll(R[0]);
+      R[1] = warp_sum_ll(R[1]);
+      R[2] = warp_sum_ll(R[2]);
+      if (lane == 0 && (R[0] | R[1] | R[2])) acc_add(x, j, R);
+    }
+  }
+}
+
+__device__ void core_gather(Ctx& x) {
+  if (x.P->a_g == 1) core_gather_t<1, kFP64Pairs>(x);
+  else core_gather_t<2, kFP64Pairs>(x);
 }
 
 /* near molecules (those with a gas-ion or gas-vapor list entry): one thread
@@ -1211,7 +1302,7 @@ __device__ void gas_near_pass_t(Ctx& x, bool eflag, bool kick) {
   const int av = P->a_v, par = x.D->parity, nt = P->n_types, ni = P->n_ion;
   const bool gi = term_on(x, MDN_I_GI), gv = term_on(x, MDN_I_GV);
   const bool intra = term_on(x, MDN_I_GAS_INTRA) && P->n_gas_bonds > 0;
-  const bool gg = term_on(x, MDN_I_GG) && P->ggl_cap > 0;
+  const bool gg = kGG && term_on(x, MDN_I_GG) && P->ggl_cap > 0;
   const int nj = (P->quirks & MDN_Q_GV_GAS_COUNT) ? min(ag, av) : av;
   int lo, hi;
   partition(x, x.D->n_gas_in, &lo, &hi);
@@ -1254,32 +1345,16 @@ __device__ void gas_near_pass_t(Ctx& x, bool eflag, bool kick) {
     if (gi) {
       const int start = a->near_gi[ms], cnt = a->gil_n[ms];
       for (int q = 0; q < cnt; q++) {
-        int j = a->gil[P->gil_off + start + q];
-        float4 pj = x.c.pos[j];
-        int tj = x.c.type[j];
-        long long R[3] = {0, 0, 0};
+        const int j = a->gil[P->gil_off + start + q];
+        const int tj = x.c.type[j];
         for (int at = 0; at < ag; at++) {
-          long long fx, fy, fz;
-          if constexpr (FP64) {
-            const double ex = X[3 * at] - x.c.x[3 * j], ey = X[3 * at + 1] - x.c.x[3 * j + 1],
-                         ez = X[3 * at + 2] - x.c.x[3 * j + 2];
-            const double fd = lj_coul_d(ex * ex + ey * ey + ez * ez, x.db[P->d_ljA + gtype[at] * nt + tj],
-                                        x.db[P->d_ljB + gtype[at] * nt + tj], 0.0, false);
-            fx = fixd(fd * ex); fy = fixd(fd * ey); fz = fixd(fd * ez);
-          } else {
-            float dx = gp[at].x - pj.x, dy = gp[at].y - pj.y, dz = gp[at].z - pj.z;
-            float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            float ee;
-            float fp = lj_coul(r2, x.c.ljA[gtype[at] * nt + tj], x.c.ljB[gtype[at] * nt + tj], 0.0f, false, &ee);
-            fx = fixf(fp * dx); fy = fixf(fp * dy); fz = fixf(fp * dz);
-          }
-          F[at][0] += fx; F[at][1] += fy; F[at][2] += fz;
-          R[0] -= fx; R[1] -= fy; R[2] -= fz;
+          long long f[3];
+          gas_core_pair<FP64>(x, X + 3 * at, gp[at], gtype[at], j, f);
+          F[at][0] += f[0]; F[at][1] += f[1]; F[at][2] += f[2];
           if (eflag)
             egi += efixd(lj_coul_energy(r2d(X + 3 * at, x.c.x + 3 * j), x.db[P->d_ljA + gtype[at] * nt + tj],
                                         x.db[P->d_ljB + gtype[at] * nt + tj], 0.0));
         }
-        acc_add(x, j, R);
       }
     }
     if (gv) {
@@ -1287,32 +1362,16 @@ __device__ void gas_near_pass_t(Ctx& x, bool eflag, bool kick) {
       for (int ent = 0; ent < cnt; ent++) {
         const int vs = a->gvl[P->gvl_off + start + ent];
         for (int b = 0; b < nj; b++) {
-          int j = ni + vs * av + b;
-          float4 pj = x.c.pos[j];
-          int tj = x.c.type[j];
-          long long R[3] = {0, 0, 0};
+          const int j = ni + vs * av + b;
+          const int tj = x.c.type[j];
           for (int at = 0; at < ag; at++) {
-            long long fx, fy, fz;
-            if constexpr (FP64) {
-              const double ex = X[3 * at] - x.c.x[3 * j], ey = X[3 * at + 1] - x.c.x[3 * j + 1],
-                           ez = X[3 * at + 2] - x.c.x[3 * j + 2];
-              const double fd = lj_coul_d(ex * ex + ey * ey + ez * ez, x.db[P->d_ljA + gtype[at] * nt + tj],
-                                          x.db[P->d_ljB + gtype[at] * nt + tj], 0.0, false);
-              fx = fixd(fd * ex); fy = fixd(fd * ey); fz = fixd(fd * ez);
-            } else {
-              float dx = gp[at].x - pj.x, dy = gp[at].y - pj.y, dz = gp[at].z - pj.z;
-              float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-              float ee;
-              float fp = lj_coul(r2, x.c.ljA[gtype[at] * nt + tj], x.c.ljB[gtype[at] * nt + tj], 0.0f, false, &ee);
-              fx = fixf(fp * dx); fy = fixf(fp * dy); fz = fixf(fp * dz);
-            }
-            F[at][0] += fx; F[at][1] += fy; F[at][2] += fz;
-            R[0] -= fx; R[1] -= fy; R[2] -= fz;
+            long long f[3];
+            gas_core_pair<FP64>(x, X + 3 * at, gp[at], gtype[at], j, f);
+            F[at][0] += f[0]; F[at][1] += f[1]; F[at][2] += f[2];
             if (eflag)
               egv += efixd(lj_coul_energy(r2d(X + 3 * at, x.c.x + 3 * j), x.db[P->d_ljA + gtype[at] * nt + tj],
                                           x.db[P->d_ljB + gtype[at] * nt + tj], 0.0));
           }
-          acc_add(x, j, R);
         }
       }
     }
@@ -1397,6 +1456,7 @@ __device__ void core_reduce(Ctx& x, cg::cluster_group& cl) {
 __device__ void forces_and_kick(Ctx& x, cg::cluster_group& cl, bool eflag, bool kick) {
   prof_start(x);
   gas_near_pass(x, eflag, kick);
+  core_gather(x);
   __syncthreads();
   prof_end(x, MDN_PROF_NEAR);
   prof_start(x);
@@ -1426,9 +1486,22 @@ __device__ void insert_vapor(const Ctx& x, int q, int n_rebuild, int t, double* 
 
 /* true when no atom of X[0..n) lies within MDN_INSERT_MIN_DIST of a core atom
  * (ion, vapor in the domain before this rebuild) or of a vapor molecule whose
- * entry this rebuild already accepted */
+ * entry this rebuild already accepted; with the gas-gas term on, nor of a gas
+ * atom in the domain before this rebuild (gas molecules entering in the same
+ * rebuild are not tested against each other) */
 __device__ bool insert_clear(const Ctx& x, const double* X, int n, int n_rebuild) {
   const double d2min = MDN_INSERT_MIN_DIST * MDN_INSERT_MIN_DIST;
+  if (kGG && (x.P->interactions & MDN_I_GG)) {
+    const RepParams* P = x.P;
+    const int G = x.D->n_gas_in, par = x.D->parity;
+    for (int u = 0; u < G * P->a_g; u++) {
+      const double* gpos = x.a->slab_x + 3 * ((size_t)P->slab_off + (size_t)par * P->slab_cap * P->a_g + u);
+      for (int a = 0; a < n; a++) {
+        double dx = X[3 * a] - gpos[0], dy = X[3 * a + 1] - gpos[1], dz = X[3 * a + 2] - gpos[2];
+        if (dx * dx + dy * dy + dz * dz < d2min) return false;
+      }
+    }
+  }
   for (int i = 0; i < x.n_core; i++) {
     const double* c = x.c.x + 3 * i;
     for (int a = 0; a < n; a++) {
@@ -1652,6 +1725,61 @@ __device__ void relist_gg(Ctx& x, cg::cluster_group& cl) {
   cl.sync();
 }
 
+/* The gas-ion and gas-vapor lists by core partner: row j (ion atom) or
+ * n_ion + q (vapor slab slot) holds the slab slots of the near gas molecules
+ * that list it.  Counts per row, a prefix over the rows, then each molecule
+ * takes a place in each of its partners' rows; the order inside a row does
+ * not matter, since the reactions gathered from it are integer sums. */
+__device__ void transpose_lists(Ctx& x, cg::cluster_group& cl, int lo, int hi) {
+  const RepParams* P = x.P;
+  const KArgs* a = x.a;
+  const int par = x.D->parity, ni = P->n_ion, ne = ni + x.D->n_vap_in;
+  int* tst = a->tr_start + P->tr_eoff;
+  int* cur = a->tr_cur + P->tr_eoff;
+  int* ent = a->tr + P->tr_off;
+  int* sc = x.iscr;
+  if (x.rank == 0)
+    for (int e = threadIdx.x; e <= ne; e += blockDim.x) cur[e] = 0;
+  __threadfence();
+  cl.sync();
+  for (int pass = 0; pass < 2; pass++) {
+    for (int s = lo + (int)threadIdx.x; s < hi; s += blockDim.x) {
+      const size_t ms = gmol(P, par, s);
+      const int ng = a->gil_n[ms], nv = a->gvl_n[ms];
+      if (!(ng | nv)) continue;
+      const unsigned short* gl = a->gil + P->gil_off + a->near_gi[ms];
+      const unsigned short* vl = a->gvl + P->gvl_off + a->near_gv[ms];
+      for (int q = 0; q < ng + nv; q++) {
+        const int row = q < ng ? (int)gl[q] : ni + (int)vl[q - ng];
+        const int at = atomicAdd(&cur[row], 1);
+        if (pass) ent[at] = s;
+      }
+    }
+    __threadfence();
+    cl.sync();
+    if (pass == 0) {
+      /* counts -> row starts (rank 0), which the fill pass advances */
+      if (x.rank == 0) {
+        int run = 0;
+        for (int e0 = 0; e0 < ne; e0 += blockDim.x) {
+          const int e = e0 + threadIdx.x;
+          const int c = e < ne ? cur[e] : 0;
+          int t;
+          const int off = block_exscan(c, sc, &t);
+          if (e < ne) {
+            tst[e] = run + off;
+            cur[e] = run + off;
+          }
+          run += t;
+        }
+        if (threadIdx.x == 0) tst[ne] = run;
+      }
+      __threadfence();
+      cl.sync();
+    }
+  }
+}
+
 /* pair lists of the gas slab (current parity) from the centres: gas-ion
  * (PotentialGasIon::makePair) and gas-vapor (PotentialVaporGas::makePair) */
 __device__ void relist(Ctx& x, cg::cluster_group& cl) {
@@ -1766,7 +1894,8 @@ __device__ void relist(Ctx& x, cg::cluster_group& cl) {
   }
   __threadfence();
   cl.sync();
-  if (P->ggl_cap > 0 && (P->interactions & MDN_I_GG)) relist_gg(x, cl);
+  transpose_lists(x, cl, lo, hi);
+  if (kGG && P->ggl_cap > 0 && (P->interactions & MDN_I_GG)) relist_gg(x, cl);
 }
 
 /* The overlap test of entering vapor molecules: against the ion, the vapor
@@ -2094,7 +2223,7 @@ __device__ void one_step(Ctx& x, cg::cluster_group& cl, bool eflag) {
   const bool rebuild = x.D->loop_pair + 1 > x.D->loop_update;
   /* with gas-gas forces no gas molecule can take its force during its own
    * drift: they need every molecule's new position */
-  const bool gg = (P->interactions & MDN_I_GG) && P->ggl_cap > 0;
+  const bool gg = kGG && (P->interactions & MDN_I_GG) && P->ggl_cap > 0;
   core_drift_shake(x, !rebuild && !gg, eflag);
   ion_centre(x);
   if (x.D->nvt_mode == MDN_NVT_NH) {
@@ -2136,7 +2265,11 @@ __device__ void one_step(Ctx& x, cg::cluster_group& cl, bool eflag) {
 
 }  // namespace
 
-#ifdef MDN_FP64_PAIRS
+#if defined(MDN_GG_TERMS) && defined(MDN_FP64_PAIRS)
+#define MDN_ADVANCE_KERNEL mdn_advance_gg_fp64
+#elif defined(MDN_GG_TERMS)
+#define MDN_ADVANCE_KERNEL mdn_advance_gg
+#elif defined(MDN_FP64_PAIRS)
 #define MDN_ADVANCE_KERNEL mdn_advance_fp64
 #else
 #define MDN_ADVANCE_KERNEL mdn_advance

@@ -400,7 +400,7 @@ def assemble(ion: Species, gas: Species, vap: Species, *, gas_name: str, n_gas: 
              n_vap: int, T: float, p: float, dt: float, interactions: int, seed: int,
              shake_h: bool, rng: np.random.Generator, nvt_mode=abi.NVT_OFF,
              min_dist: float = 10.0, box: Optional[float] = None, label: str = "",
-             reference_masses: bool = False, placer=None) -> ReplicaSpec:
+             reference_masses: bool = False, placer=None, gas_min_dist: float = 0.0) -> ReplicaSpec:
     """Concatenates the species' tables (ion, gas, vapor order), places the
     molecules uniformly in the cube and draws Maxwell-Boltzmann velocities.
 
@@ -453,7 +453,7 @@ def assemble(ion: Species, gas: Species, vap: Species, *, gas_name: str, n_gas: 
     if placer is not None:
         gx, gv, vx, vv = placer(box, ion_top.x, n_gas, n_vap, mb_sigma(T, gas_m), mb_sigma(T, vap_m), seed)
     else:
-        gx, gv, vx, vv = _place(rng, box, ion_top.x, n_gas, n_vap, min_dist, mb_sigma(T, gas_m),
+        gx, gv, vx, vv = _place(rng, box, ion_top.x, n_gas, n_vap, min_dist, gas_min_dist, mb_sigma(T, gas_m),
                                 mb_sigma(T, vap_m))
     bmh = ion.bmh if ion.bmh is not None else np.zeros(ion_top.n, np.int32)
     return ReplicaSpec(
@@ -468,10 +468,12 @@ def assemble(ion: Species, gas: Species, vap: Species, *, gas_name: str, n_gas: 
         seed=seed, pressure=p, label=label)
 
 
-def _place(rng, box, ion_x, n_gas, n_vap, min_dist, gas_sigma, vap_sigma):
+def _place(rng, box, ion_x, n_gas, n_vap, min_dist, gas_min_dist, gas_sigma, vap_sigma):
     """Centres uniform in the cube: vapor first, each min_dist from the ion
     atoms' bounding sphere and from the vapor already placed, then the gas
-    (min_dist from the ion and the vapor); Maxwell-Boltzmann velocities."""
+    (min_dist from the ion and the vapor, and gas_min_dist from each other
+    when it is positive: systems with the gas-gas term need it);
+    Maxwell-Boltzmann velocities."""
     half = box / 2
     ion_r = np.linalg.norm(ion_x, axis=1).max() if len(ion_x) else 0.0
     vx = []
@@ -499,7 +501,10 @@ def _place(rng, box, ion_x, n_gas, n_vap, min_dist, gas_sigma, vap_sigma):
             for b in range(0, len(c), 4096):
                 d = np.linalg.norm(c[b:b + 4096, None, :] - vx[None], axis=2).min(axis=1)
                 ok[b:b + 4096] &= d >= min_dist
-        gx = np.concatenate([gx, c[ok]])[:n_gas]
+        c = c[ok]
+        if gas_min_dist > 0:
+            c = _thin(c, gx, gas_min_dist, box)
+        gx = np.concatenate([gx, c])[:n_gas]
     gv = rng.normal(size=(n_gas, 3)) * gas_sigma
     vv = rng.normal(size=(n_vap, 3)) * vap_sigma
     return gx, gv, vx, vv
@@ -513,6 +518,38 @@ def _shift(arr, width, col, off):
 
 
 BASE_TERMS = abi.I_GI | abi.I_GV | abi.I_VI | abi.I_VV | abi.I_GAS_INTRA | abi.I_VAPOR_INTRA
+
+
+def _thin(cand, placed, d, box):
+    """The candidates, in order, that lie at least d from every placed centre
+    and every earlier kept candidate (minimum image in the periodic cube)."""
+    cells = {}
+    n = max(1, int(box // d))
+    w = box / n
+
+    def key(p):
+        return tuple(int(np.floor((p[k] + box / 2) / w)) % n for k in range(3))
+
+    def clear(p):
+        kx, ky, kz = key(p)
+        for i in (-1, 0, 1):
+            for j in (-1, 0, 1):
+                for k in (-1, 0, 1):
+                    for q in cells.get(((kx + i) % n, (ky + j) % n, (kz + k) % n), ()):
+                        dv = p - q
+                        dv -= box * np.round(dv / box)
+                        if dv @ dv < d * d:
+                            return False
+        return True
+
+    for p in placed:
+        cells.setdefault(key(p), []).append(p)
+    keep = []
+    for p in cand:
+        if clear(p):
+            cells.setdefault(key(p), []).append(p)
+            keep.append(p)
+    return np.array(keep).reshape(-1, 3)
 
 
 def config0(replica: int = 0, n_gas: int = 2000, n_vap: int = 20) -> ReplicaSpec:
@@ -531,6 +568,37 @@ def config1(replica: int = 0, n_gas: int = 100_000, n_vap: int = 100, chain_atom
                     n_gas=n_gas, n_vap=n_vap, T=300.0, p=1e5, dt=1.0,
                     interactions=BASE_TERMS | abi.I_AMBER | abi.I_SHAKE,
                     seed=seed_of(1, replica), shake_h=True, rng=rng, label="config1")
+
+
+def config3(replica: int = 0, n_near: int = 8, r_lo: float = 8.0, r_hi: float = 28.0, margin: float = 40.0,
+            **kw) -> ReplicaSpec:
+    """The adjoint window's system: configuration 1 with n_near of its
+    methanol molecules moved to centres r_lo..r_hi A from the chain's
+    centre (each at least 6 A from every chain atom and 8 A from each other),
+    so that the window's ion-vapor energy and smooth count are not
+    identically zero (at 1e5 Pa and 100 molecules in the 1,606 A box the
+    domain holds 0.13 methanol on average).  The list margin is raised so
+    that the window holds no effective-domain rebuild."""
+    spec = config1(replica, **kw)
+    rng = np.random.default_rng(seed_of(3, replica))
+    ion_x = spec.ion.x
+    placed = []
+    tries = 0
+    while len(placed) < n_near:
+        tries += 1
+        if tries > 100000:
+            raise RuntimeError("could not place the near methanol")
+        d = rng.normal(size=3)
+        c = d / np.linalg.norm(d) * rng.uniform(r_lo, r_hi)
+        if np.linalg.norm(ion_x - c, axis=1).min() < 6.0:
+            continue
+        if placed and np.linalg.norm(np.array(placed) - c, axis=1).min() < 8.0:
+            continue
+        placed.append(c)
+    spec.vapor_x[:n_near] = np.array(placed)
+    spec.margin = margin
+    spec.label = "config3"
+    return spec
 
 
 def config2_replica(replica: int, scale: float = 1.0) -> ReplicaSpec:
@@ -586,9 +654,10 @@ def config4_replica(replica: int = 0, n_gas: int = 1_000_000, n_vap: int = 1000,
 def small_system(seed: int = 7, gas: str = "N2", vapor: str = "methanol", ion: str = "nacl",
                  n_gas: int = 400, n_vap: int = 12, box: float = 260.0, interactions=None,
                  shake_h: bool = False, rigid_gas: bool = False, chain_atoms: int = 30,
-                 nvt_mode=abi.NVT_OFF, dt: float = 1.0) -> ReplicaSpec:
+                 nvt_mode=abi.NVT_OFF, dt: float = 1.0, gas_min_dist: float = 0.0) -> ReplicaSpec:
     """A small replica for parity tests: a dense gas in a small box so that
-    the sphere holds many molecules."""
+    the sphere holds many molecules (gas centres gas_min_dist apart when it
+    is positive)."""
     rng = np.random.default_rng(seed)
     ion_sp = nacl_cluster() if ion == "nacl" else chain(chain_atoms, 1.0, rng)
     vap_sp = methanol() if vapor == "methanol" else water()
@@ -601,7 +670,8 @@ def small_system(seed: int = 7, gas: str = "N2", vapor: str = "methanol", ion: s
     return assemble(ion_sp, gas_species(gas, rigid=rigid_gas), vap_sp, gas_name=gas,
                     n_gas=n_gas, n_vap=n_vap, T=300.0, p=p, dt=dt, interactions=interactions,
                     seed=seed, shake_h=shake_h, rng=rng, nvt_mode=nvt_mode,
-                    min_dist=min(10.0, 0.5 * n_dens ** (-1 / 3)), box=box, label="small")
+                    min_dist=min(10.0, 0.5 * n_dens ** (-1 / 3)), box=box, label="small",
+                    gas_min_dist=gas_min_dist)
 
 
 # --------------------------------------------------------------------------

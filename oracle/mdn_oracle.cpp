@@ -408,6 +408,14 @@ struct Oracle {
         double dx = X[a][0] - c[0], dy = X[a][1] - c[1], dz = X[a][2] - c[2];
         if (dx * dx + dy * dy + dz * dz < d2min) return false;
       }
+    /* with the gas-gas term on, an entering gas molecule is also tested
+     * against the gas in the domain before this rebuild */
+    if (!vapor && (I & MDN_I_GG))
+      for (const V3& c : gas_before)
+        for (int a = 0; a < n; a++) {
+          double dx = X[a][0] - c[0], dy = X[a][1] - c[1], dz = X[a][2] - c[2];
+          if (dx * dx + dy * dy + dz * dz < d2min) return false;
+        }
     return true;
   }
 

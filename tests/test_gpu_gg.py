@@ -21,7 +21,10 @@ NAMES = ["nacl_n2_meoh", "chain_he_water"]
 
 
 def gg_system(name):
-    return systems.with_terms(systems.make(name), extra=abi.I_GG)
+    """gas centres at least 4 A apart: the placement (like the reference's,
+    src/initialization/initializationGas.cpp:36-56) keeps molecules only
+    clear of the ion, which gas that does not interact with itself allows"""
+    return systems.with_terms(systems.make(name, gas_min_dist=4.0), extra=abi.I_GG)
 
 
 @pytest.fixture(scope="module")
@@ -75,11 +78,13 @@ def test_gg_fp64_pair_mode_forces(eng, oracle_libs, name):
     assert err <= 1e-9, f"relative RMS force error {err:.2e}"
 
 
-@pytest.mark.parametrize("quirks", [pytest.param(abi.Q_ALL, id="blind"), pytest.param(CHECKED, id="checked")])
 @pytest.mark.parametrize("name", NAMES)
-def test_gg_trajectory_across_rebuild(eng, oracle_libs, name, quirks):
-    """30 steps with a rebuild at the first step: molecules entering then
-    carry taper weight 0 for that step in both."""
+def test_gg_trajectory_across_rebuild(eng, oracle_libs, name):
+    """30 steps with a rebuild at the first step, checked insertion (which
+    with the gas-gas term also keeps entering gas 2 A from the gas in the
+    domain; the reference's blind insertion can drop one gas molecule onto
+    another): molecules entering carry taper weight 0 for that step in both."""
+    quirks = CHECKED
     spec = gg_system(name)
     o = oracle_libs.OracleReplica(spec, quirks=quirks)
     o.step(2)
