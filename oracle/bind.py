@@ -198,6 +198,10 @@ def orc_lib():
         L.orc_step_many.argtypes = [C.POINTER(vp), C.c_int, C.c_longlong, C.c_int]
         L.orc_objective.restype = C.c_double
         L.orc_objective.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_double]
+        L.orc_adjoint.restype = C.c_int
+        L.orc_adjoint.argtypes = [vp, C.c_longlong, C.c_double, C.c_double, C.c_double, C.c_double,
+                                  C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_double),
+                                  C.POINTER(C.c_double)]
         L.orc_window.restype = C.c_double
         L.orc_window.argtypes = [vp, C.c_longlong, C.c_double, C.c_double, C.c_double, C.c_double]
         dp = C.POINTER(C.c_double)
@@ -299,6 +303,20 @@ class OracleReplica:
 
     def objective(self, R0=10.0, W=1.0, w_energy=1.0, w_count=1.0):
         return self.L.orc_objective(self.h, R0, W, w_energy, w_count)
+
+    def adjoint(self, n, theta, rows, R0=10.0, W=1.0, w_energy=1.0, w_count=1.0):
+        """(J, dJ/dtheta) of the window over the next n steps by the FP64 CPU
+        adjoint (oracle/adjoint_ad.h); the replica is not advanced.  theta,
+        rows: as gradients.parameters (rows as mdn_adjoint_params)."""
+        th = np.ascontiguousarray(theta, np.float64)
+        rw = np.ascontiguousarray(rows, np.int32).reshape(-1, 3)
+        J = C.c_double(0.0)
+        g = np.zeros(len(th))
+        rc = self.L.orc_adjoint(self.h, n, R0, W, w_energy, w_count, abi.ptr(th), abi.ptr(rw, C.c_int), len(rw),
+                                C.byref(J), abi.ptr(g))
+        if rc != 0:
+            raise RuntimeError(f"orc_adjoint returned {rc}")
+        return J.value, g
 
     def window(self, n, R0=10.0, W=1.0, w_energy=1.0, w_count=1.0):
         """Advances n steps; the window average of the objective."""

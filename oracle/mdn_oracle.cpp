@@ -1040,6 +1040,10 @@ Oracle* create(const mdn_replica_desc* d, unsigned quirks, int force_mode) {
   return o;
 }
 
+/* the FP64 CPU adjoint of the gradient harness (reverse-mode differentiation
+ * of the window's steps) */
+#include "adjoint_ad.h"
+
 }  // namespace
 
 extern "C" {
@@ -1204,6 +1208,16 @@ double orc_objective(void* h, double R0, double W, double we, double wc) {
 
 /* Advances n steps and returns the window average of the objective after
  * each step: the quantity mdn_adjoint differentiates. */
+/* The window objective over the next n steps and its gradient by the FP64
+ * CPU adjoint (adjoint_ad.h); theta / rows as mdn_adjoint_params (nrows rows,
+ * 2 (nrows - 1) + 1 parameters, the values the replica was built with).
+ * Returns 0, -1 for a window mdn_adjoint refuses too, -2 when SHAKE did not
+ * converge.  The replica is not advanced. */
+int orc_adjoint(void* h, long long n, double R0, double W, double we, double wc, const double* theta,
+                const int* rows, int nrows, double* J, double* grad) {
+  return adj::window_adjoint(*(Oracle*)h, n, R0, W, we, wc, theta, rows, nrows, J, grad);
+}
+
 double orc_window(void* h, long long n, double R0, double W, double we, double wc) {
   Oracle* o = (Oracle*)h;
   double s = 0;

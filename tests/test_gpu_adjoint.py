@@ -166,3 +166,26 @@ def test_adjoint_on_the_config3_window(eng, oracle_libs):
             Jk.append(o.window(w["n_steps"], w["count_radius"], w["count_width"], w["w_energy"], w["w_count"]))
         fd[k] = (Jk[0] - Jk[1]) / (2 * h)
     check(grad, fd, 1e-4, floor=1e-2)
+
+
+@pytest.mark.parametrize("shake", [False, True])
+def test_adjoint_matches_the_cpu_adjoint(eng, oracle_libs, shake):
+    """The engine's adjoint (hand-written transposes, the adjoint of the
+    converged SHAKE projection) against the FP64 CPU adjoint (reverse-mode
+    differentiation of the oracle's step, oracle/adjoint_ad.h) on the same
+    window with the FP64 forward: J within 1e-9 and every derivative within
+    1e-6 relative (1e-5 with SHAKE, differentiated through its iterations on
+    the CPU), below 1e-4 of the largest within 1e-6 of that floor."""
+    from md_nucleation_b200.gradients import parameters
+    spec = system(shake)
+    theta0, rows = parameters(spec)
+    e = eng.Engine([spec], force_mode=1)
+    J, grad, _ = e.adjoint(**WINDOW)
+    kw = dict(R0=WINDOW["count_radius"], W=WINDOW["count_width"], w_energy=WINDOW["w_energy"],
+              w_count=WINDOW["w_count"])
+    Jc, gc = oracle_libs.OracleReplica(spec).adjoint(WINDOW["n_steps"], theta0.numpy(), rows, **kw)
+    assert abs(J - Jc) <= 1e-9 * max(abs(Jc), 1.0)
+    tol = 1e-5 if shake else 1e-6
+    floor = 1e-4 * np.abs(gc).max()
+    for k in range(len(gc)):
+        assert abs(grad[k] - gc[k]) <= tol * max(abs(gc[k]), floor), f"parameter {k}: {grad[k]} vs {gc[k]}"
