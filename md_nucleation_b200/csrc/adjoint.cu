@@ -683,23 +683,15 @@ __device__ void shake_adjoint(const Sys& S, const Buf& B, const double* x, const
   __syncthreads();
 }
 
-/* One segment: recompute K steps from (X[0], V[0]), then walk them back.
- * first = 1 for the window's first segment: its start forces are the ones
- * the state holds (f0; zero on a replica that was never stepped, since the
- * reference evaluates no force before the first kick), and f0_theta = 1 when
- * they came from a force evaluation at x_0, whose parameter dependence then
- * enters the gradient.  Other segments recompute F(x_0) and leave the force
- * adjoint at their start in lf for the previous segment. */
-__global__ void __launch_bounds__(ADJ_THREADS, 1) adjoint_segment(Sys S, Buf B, int K, int first,
-                                                                  const double* f0, int f0_theta) {
-  __shared__ double sgrad[MAX_PARAMS];
-  __shared__ double red[40];
-  __shared__ double cent[3];
+/* The FP64 recompute of one segment: K steps from (X[0], V[0]), keeping x,
+ * v, F and the converged SHAKE multipliers of every step; returns the
+ * segment's sum of the objective.  first = 1 for the window's first segment,
+ * whose start forces are the ones the state holds (f0; zero on a replica
+ * that was never stepped, since the reference evaluates no force before the
+ * first kick); other segments evaluate F(x_0). */
+__device__ double recompute(const Sys& S, const Buf& B, int K, int first, const double* f0, double* red,
+                            double* cent) {
   const int n3 = 3 * S.N;
-  for (int p = threadIdx.x; p < S.n_params; p += blockDim.x) sgrad[p] = 0;
-  if (threadIdx.x == 0) B.flag[1] = 0;
-  __syncthreads();
-  /* ---- recompute ---- */
   if (first) {
     for (int q = threadIdx.x; q < n3; q += blockDim.x) B.F[q] = f0[q];
     __syncthreads();
@@ -712,13 +704,13 @@ __global__ void __launch_bounds__(ADJ_THREADS, 1) adjoint_segment(Sys S, Buf B, 
   for (int t = 1; t <= K; t++) {
     const double* x0 = B.X + (size_t)(t - 1) * n3;
     const double* v0 = B.V + (size_t)(t - 1) * n3;
-    const double* f0 = B.F + (size_t)(t - 1) * n3;
+    const double* f0t = B.F + (size_t)(t - 1) * n3;
     double* x1 = B.X + (size_t)t * n3;
     double* v1 = B.V + (size_t)t * n3;
     double* f1 = B.F + (size_t)t * n3;
     for (int q = threadIdx.x; q < n3; q += blockDim.x) {
       const int i = q / 3;
-      double va = v0[q] + S.c[i] * f0[q];
+      double va = v0[q] + S.c[i] * f0t[q];
       v1[q] = va;
       x1[q] = x0[q] + S.dt * va;
     }
@@ -739,9 +731,54 @@ __global__ void __launch_bounds__(ADJ_THREADS, 1) adjoint_segment(Sys S, Buf B, 
     __syncthreads();
     jacc += objective(S, x1, nullptr, nullptr, cent, false);
   }
-  jacc = block_sum(jacc, red);
-  if (threadIdx.x == 0) B.J[0] += jacc * S.inv_n;
-  /* ---- backward ---- */
+  return block_sum(jacc, red);
+}
+
+/* Every segment's recompute at once, one CTA each: CTA s starts from
+ * checkpoint s (cpx, cpv) and writes its segment's trajectory at
+ * B.X/V/F/gam + s * stride; its scratch (weights, SHAKE flags) at its own
+ * offsets; Jseg[s] = the segment's objective sum, flags[2 s + 1] its
+ * SHAKE status. */
+__global__ void __launch_bounds__(ADJ_THREADS, 1) adjoint_recompute(Sys S, Buf B, int K, long long n_steps,
+                                                                    const double* cpx, const double* cpv,
+                                                                    const double* f0, double* Jseg) {
+  __shared__ double red[40];
+  __shared__ double cent[3];
+  const int s = blockIdx.x;
+  const int n3 = 3 * S.N;
+  const int Ks = (int)min((long long)K, n_steps - (long long)s * K);
+  Buf b = B;
+  const size_t xs = (size_t)(K + 1) * n3;
+  b.X += s * xs;
+  b.V += s * xs;
+  b.F += s * xs;
+  b.gam += (size_t)s * K * max(S.n_cons, 1);
+  b.w += (size_t)s * S.N;
+  b.dw += (size_t)s * n3;
+  b.flag += 2 * s;
+  for (int q = threadIdx.x; q < n3; q += blockDim.x) {
+    b.X[q] = cpx[(size_t)s * n3 + q];
+    b.V[q] = cpv[(size_t)s * n3 + q];
+  }
+  if (threadIdx.x == 0) b.flag[1] = 0;
+  __syncthreads();
+  const double j = recompute(S, b, Ks, s == 0 ? 1 : 0, f0, red, cent);
+  if (threadIdx.x == 0) Jseg[s] = j;
+}
+
+/* The reverse sweep of one segment over its recomputed trajectory (B
+ * pointing at it), last step first; the adjoints of x, v, F carry over from
+ * the segment after it.  f0_theta = 1 on the first segment when its start
+ * forces came from a force evaluation at x_0, whose parameter dependence
+ * then enters the gradient. */
+__global__ void __launch_bounds__(ADJ_THREADS, 1) adjoint_segment(Sys S, Buf B, int K, int first,
+                                                                  int f0_theta) {
+  __shared__ double sgrad[MAX_PARAMS];
+  __shared__ double red[40];
+  __shared__ double cent[3];
+  const int n3 = 3 * S.N;
+  for (int p = threadIdx.x; p < S.n_params; p += blockDim.x) sgrad[p] = 0;
+  __syncthreads();
   for (int t = K; t >= 1; t--) {
     const double* x0 = B.X + (size_t)(t - 1) * n3;
     const double* x1 = B.X + (size_t)t * n3;
@@ -1121,22 +1158,24 @@ extern "C" int mdn_adjoint(mdn_handle* h, const mdn_replica_desc* d, const mdn_a
   const size_t n3 = 3 * (size_t)N;
   Buf Bf;
   memset(&Bf, 0, sizeof Bf);
-  Bf.X = dzero<double>((K + 1) * n3, owned);
-  Bf.V = dzero<double>((K + 1) * n3, owned);
-  Bf.F = dzero<double>((K + 1) * n3, owned);
-  Bf.gam = dzero<double>((size_t)K * std::max(ncons, 1), owned);
+  /* every segment's recomputed trajectory (the recomputes run at once) */
+  Bf.X = dzero<double>((size_t)nseg * (K + 1) * n3, owned);
+  Bf.V = dzero<double>((size_t)nseg * (K + 1) * n3, owned);
+  Bf.F = dzero<double>((size_t)nseg * (K + 1) * n3, owned);
+  Bf.gam = dzero<double>((size_t)nseg * K * std::max(ncons, 1), owned);
   Bf.lx = dzero<double>(n3, owned);
   Bf.lv = dzero<double>(n3, owned);
   Bf.lf = dzero<double>(n3, owned);
   Bf.tmp = dzero<double>(n3, owned);
   Bf.xb = dzero<double>(n3, owned);
-  Bf.w = dzero<double>(N, owned);
-  Bf.dw = dzero<double>(n3, owned);
+  Bf.w = dzero<double>((size_t)nseg * N, owned);
+  Bf.dw = dzero<double>((size_t)nseg * n3, owned);
   Bf.om = dzero<double>(N, owned);
   Bf.mu = dzero<double>(std::max(ncons, 1), owned);
   Bf.grad = dzero<double>(n_params, owned);
   Bf.J = dzero<double>(1, owned);
-  Bf.flag = dzero<int>(2, owned);
+  Bf.flag = dzero<int>(2 * (size_t)nseg, owned);
+  double* d_jseg = dzero<double>(nseg, owned);
   /* the forces the state holds at the window start */
   std::vector<double> f0(3 * (size_t)N, 0.0);
   for (int i = 0; i < ni; i++)
@@ -1200,11 +1239,15 @@ extern "C" int mdn_adjoint(mdn_handle* h, const mdn_replica_desc* d, const mdn_a
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0, stream);
+  adjoint_recompute<<<(unsigned)nseg, ADJ_THREADS, 0, stream>>>(S, Bf, K, spec->n_steps, cpx, cpv, d_f0, d_jseg);
   for (long long s = nseg - 1; s >= 0; s--) {
     const int n = (int)std::min<long long>(K, spec->n_steps - s * K);
-    cudaMemcpyAsync(Bf.X, cpx + s * n3, sizeof(double) * n3, cudaMemcpyDeviceToDevice, stream);
-    cudaMemcpyAsync(Bf.V, cpv + s * n3, sizeof(double) * n3, cudaMemcpyDeviceToDevice, stream);
-    adjoint_segment<<<1, ADJ_THREADS, 0, stream>>>(S, Bf, n, s == 0 ? 1 : 0, d_f0, f0_theta);
+    Buf b = Bf;
+    b.X += s * (K + 1) * n3;
+    b.V += s * (K + 1) * n3;
+    b.F += s * (K + 1) * n3;
+    b.gam += (size_t)s * K * std::max(ncons, 1);
+    adjoint_segment<<<1, ADJ_THREADS, 0, stream>>>(S, b, n, s == 0 ? 1 : 0, f0_theta);
   }
   cudaEventRecord(e1, stream);
   cudaError_t ce = cudaStreamSynchronize(stream);
@@ -1216,9 +1259,17 @@ extern "C" int mdn_adjoint(mdn_handle* h, const mdn_replica_desc* d, const mdn_a
     cleanup();
     return err(MDN_ERR_CUDA, "mdn_adjoint: %s", cudaGetErrorString(ce));
   }
+  std::vector<int> fl(2 * (size_t)nseg, 0);
+  cudaMemcpy(fl.data(), Bf.flag, sizeof(int) * fl.size(), cudaMemcpyDeviceToHost);
   int flags[2] = {0, 0};
-  cudaMemcpy(flags, Bf.flag, sizeof flags, cudaMemcpyDeviceToHost);
-  cudaMemcpy(J, Bf.J, sizeof(double), cudaMemcpyDeviceToHost);
+  for (long long s = 0; s < nseg; s++) flags[1] |= fl[2 * s + 1];
+  /* J: the segments' objective sums, last first (the order the sequential
+   * form added them in) */
+  std::vector<double> js((size_t)nseg, 0.0);
+  cudaMemcpy(js.data(), d_jseg, sizeof(double) * nseg, cudaMemcpyDeviceToHost);
+  double jsum = 0.0;
+  for (long long s = nseg - 1; s >= 0; s--) jsum += js[s] * S.inv_n;
+  *J = jsum;
   cudaMemcpy(grad, Bf.grad, sizeof(double) * n_params, cudaMemcpyDeviceToHost);
   if (ms) {
     ms[0] = fwd_ms;

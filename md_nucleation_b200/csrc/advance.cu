@@ -1132,7 +1132,7 @@ __device__ void gas_gg_pass_t(Ctx& x, bool eflag, bool fresh) {
   long long egg = 0;
   for (int s = lo + (int)threadIdx.x; s < hi; s += blockDim.x) {
     const size_t ms = gmol(P, par, s);
-    const bool s_new = fresh && a->slab_ins[ms] == nreb;
+    const bool s_new = fresh && __ldcg(a->slab_ins + ms) == nreb;
     double X[3 * AG], w[AG];
 #pragma unroll
     for (int at = 0; at < AG; at++) {
@@ -1146,11 +1146,13 @@ __device__ void gas_gg_pass_t(Ctx& x, bool eflag, bool fresh) {
     const int start = a->ggl_start[ms], cnt = a->ggl_n[ms];
     for (int q = 0; q < cnt; q++) {
       const int t = a->ggl[P->ggl_off + start + q];
-      const bool t_new = fresh && a->slab_ins[gmol(P, par, t)] == nreb;
+      const bool t_new = fresh && __ldcg(a->slab_ins + gmol(P, par, t)) == nreb;
 #pragma unroll
       for (int b = 0; b < AG; b++) {
         const size_t gt = gatom(P, par, t, b);
-        const double Y[3] = {a->slab_x[3 * gt], a->slab_x[3 * gt + 1], a->slab_x[3 * gt + 2]};
+        /* another CTA's molecule, moved this step: from L2 */
+        const double Y[3] = {__ldcg(a->slab_x + 3 * gt), __ldcg(a->slab_x + 3 * gt + 1),
+                             __ldcg(a->slab_x + 3 * gt + 2)};
         const double wb = t_new ? 0.0 : taper(P, com, Y);
         const int tb = gtype[b];
 #pragma unroll
@@ -1239,7 +1241,10 @@ __device__ __forceinline__ void gas_core_pair(const Ctx& x, const double* Xa, fl
  * per row of the transposed lists (an ion atom, or a vapor molecule and each
  * of its first nj atoms), its lanes over the row's gas molecules, the sum
  * reduced across the warp and added to the core sums once.  The rows are
- * spread over the cluster's warps. */
+ * spread over the cluster's warps.  The gas positions (moved this step) and
+ * the rows (built at the last rebuild) were written by any CTA of the
+ * cluster, so they are read from L2 (__ldcg): this SM's L1 may still hold
+ * the lines as it read them before. */
 template <int AG, bool FP64>
 __device__ void core_gather_t(Ctx& x) {
   const RepParams* P = x.P;
@@ -1258,17 +1263,18 @@ __device__ void core_gather_t(Ctx& x) {
   for (int row = x.rank * nw + (int)(threadIdx.x >> 5); row < ne; row += x.C * nw) {
     const bool ion_row = row < ni;
     if (ion_row ? !gi : !gv) continue;
-    const int r0 = tst[row], rn = tst[row + 1] - r0;
+    const int r0 = __ldcg(tst + row), rn = __ldcg(tst + row + 1) - r0;
     const int nb = ion_row ? 1 : nj;
     for (int b = 0; b < nb; b++) {
       const int j = ion_row ? row : ni + (row - ni) * av + b;
       long long R[3] = {0, 0, 0};
       for (int q = lane; q < rn; q += 32) {
-        const int s = ent[r0 + q];
+        const int s = __ldcg(ent + r0 + q);
 #pragma unroll
         for (int at = 0; at < AG; at++) {
           const size_t g = gatom(P, par, s, at);
-          const double X[3] = {a->slab_x[3 * g], a->slab_x[3 * g + 1], a->slab_x[3 * g + 2]};
+          const double X[3] = {__ldcg(a->slab_x + 3 * g), __ldcg(a->slab_x + 3 * g + 1),
+                               __ldcg(a->slab_x + 3 * g + 2)};
           const float3 gp = make_float3((float)(X[0] - com[0]), (float)(X[1] - com[1]), (float)(X[2] - com[2]));
           long long f[3];
           gas_core_pair<FP64>(x, X, gp, gtype[at], j, f);
@@ -1496,8 +1502,9 @@ __device__ bool insert_clear(const Ctx& x, const double* X, int n, int n_rebuild
     const int G = x.D->n_gas_in, par = x.D->parity;
     for (int u = 0; u < G * P->a_g; u++) {
       const double* gpos = x.a->slab_x + 3 * ((size_t)P->slab_off + (size_t)par * P->slab_cap * P->a_g + u);
+      const double g0 = __ldcg(gpos), g1 = __ldcg(gpos + 1), g2 = __ldcg(gpos + 2);
       for (int a = 0; a < n; a++) {
-        double dx = X[3 * a] - gpos[0], dy = X[3 * a + 1] - gpos[1], dz = X[3 * a + 2] - gpos[2];
+        double dx = X[3 * a] - g0, dy = X[3 * a + 1] - g1, dz = X[3 * a + 2] - g2;
         if (dx * dx + dy * dy + dz * dz < d2min) return false;
       }
     }
@@ -1680,13 +1687,15 @@ __device__ void relist_gg(Ctx& x, cg::cluster_group& cl) {
   int* sc = x.iscr;
   const double* cen = a->mol_x + 3 * ((size_t)P->mol_off + 1);
   const int* smol = a->slab_mol + gmol(P, par, 0);
+  /* centres and slab entries of every CTA's molecules, from L2 */
   auto partners = [&](int s, int* out) {
-    const double* c = cen + 3 * (size_t)smol[s];
+    const double* c = cen + 3 * (size_t)__ldcg(smol + s);
+    const double c0 = __ldcg(c), c1 = __ldcg(c + 1), c2 = __ldcg(c + 2);
     int n = 0;
     for (int t = 0; t < G; t++) {
       if (t == s) continue;
-      const double* d = cen + 3 * (size_t)smol[t];
-      const double dx = c[0] - d[0], dy = c[1] - d[1], dz = c[2] - d[2];
+      const double* d = cen + 3 * (size_t)__ldcg(smol + t);
+      const double dx = c0 - __ldcg(d), dy = c1 - __ldcg(d + 1), dz = c2 - __ldcg(d + 2);
       if ((dx * dx + dy * dy + dz * dz) < P->ml2) {
         if (out) out[n] = t;
         n++;
@@ -1763,7 +1772,7 @@ __device__ void transpose_lists(Ctx& x, cg::cluster_group& cl, int lo, int hi) {
         int run = 0;
         for (int e0 = 0; e0 < ne; e0 += blockDim.x) {
           const int e = e0 + threadIdx.x;
-          const int c = e < ne ? cur[e] : 0;
+          const int c = e < ne ? __ldcg(cur + e) : 0;
           int t;
           const int off = block_exscan(c, sc, &t);
           if (e < ne) {
@@ -1799,18 +1808,20 @@ __device__ void relist(Ctx& x, cg::cluster_group& cl) {
     int s = s0 + threadIdx.x;
     int cgi = 0, cgv = 0;
     if (s < hi) {
-      int m = a->slab_mol[gmol(P, par, s)];
+      int m = __ldcg(a->slab_mol + gmol(P, par, s));
       const double* cm = a->mol_x + 3 * ((size_t)P->mol_off + 1 + m);
+      /* centres set by whichever CTA classified the molecule: from L2 */
+      const double cx0 = __ldcg(cm), cx1 = __ldcg(cm + 1), cx2 = __ldcg(cm + 2);
       if (gi)
         for (int j = 0; j < ni; j++) {
-          double dx = cm[0] - x.c.x[3 * j], dy = cm[1] - x.c.x[3 * j + 1], dz = cm[2] - x.c.x[3 * j + 2];
+          double dx = cx0 - x.c.x[3 * j], dy = cx1 - x.c.x[3 * j + 1], dz = cx2 - x.c.x[3 * j + 2];
           if ((dx * dx + dy * dy + dz * dz) < P->ml2) cgi++;
         }
       if (gv)
         for (int q = 0; q < nv; q++) {
-          int vm = a->vslab_mol[vmol(P, par, q)];
+          int vm = __ldcg(a->vslab_mol + vmol(P, par, q));
           const double* vc = a->mol_x + 3 * ((size_t)P->mol_off + 1 + P->n_gas + vm);
-          double dx = cm[0] - vc[0], dy = cm[1] - vc[1], dz = cm[2] - vc[2];
+          double dx = cx0 - __ldcg(vc), dy = cx1 - __ldcg(vc + 1), dz = cx2 - __ldcg(vc + 2);
           if ((dx * dx + dy * dy + dz * dz) < P->ml2) cgv++;
         }
     }
@@ -1832,19 +1843,23 @@ __device__ void relist(Ctx& x, cg::cluster_group& cl) {
     int s = s0 + threadIdx.x;
     int cgi = 0, cgv = 0;
     const double* cm = nullptr;
+    double cx0 = 0, cx1 = 0, cx2 = 0;
     if (s < hi) {
-      int m = a->slab_mol[gmol(P, par, s)];
+      int m = __ldcg(a->slab_mol + gmol(P, par, s));
       cm = a->mol_x + 3 * ((size_t)P->mol_off + 1 + m);
+      cx0 = __ldcg(cm);
+      cx1 = __ldcg(cm + 1);
+      cx2 = __ldcg(cm + 2);
       if (gi)
         for (int j = 0; j < ni; j++) {
-          double dx = cm[0] - x.c.x[3 * j], dy = cm[1] - x.c.x[3 * j + 1], dz = cm[2] - x.c.x[3 * j + 2];
+          double dx = cx0 - x.c.x[3 * j], dy = cx1 - x.c.x[3 * j + 1], dz = cx2 - x.c.x[3 * j + 2];
           if ((dx * dx + dy * dy + dz * dz) < P->ml2) cgi++;
         }
       if (gv)
         for (int q = 0; q < nv; q++) {
-          int vm = a->vslab_mol[vmol(P, par, q)];
+          int vm = __ldcg(a->vslab_mol + vmol(P, par, q));
           const double* vc = a->mol_x + 3 * ((size_t)P->mol_off + 1 + P->n_gas + vm);
-          double dx = cm[0] - vc[0], dy = cm[1] - vc[1], dz = cm[2] - vc[2];
+          double dx = cx0 - __ldcg(vc), dy = cx1 - __ldcg(vc + 1), dz = cx2 - __ldcg(vc + 2);
           if ((dx * dx + dy * dy + dz * dz) < P->ml2) cgv++;
         }
     }
@@ -1865,15 +1880,15 @@ __device__ void relist(Ctx& x, cg::cluster_group& cl) {
         int w = 0;
         if (gi)
           for (int j = 0; j < ni; j++) {
-            double dx = cm[0] - x.c.x[3 * j], dy = cm[1] - x.c.x[3 * j + 1], dz = cm[2] - x.c.x[3 * j + 2];
+            double dx = cx0 - x.c.x[3 * j], dy = cx1 - x.c.x[3 * j + 1], dz = cx2 - x.c.x[3 * j + 2];
             if ((dx * dx + dy * dy + dz * dz) < P->ml2) a->gil[P->gil_off + bgi + w++] = (unsigned short)j;
           }
         w = 0;
         if (gv)
           for (int q = 0; q < nv; q++) {
-            int vm = a->vslab_mol[vmol(P, par, q)];
+            int vm = __ldcg(a->vslab_mol + vmol(P, par, q));
             const double* vc = a->mol_x + 3 * ((size_t)P->mol_off + 1 + P->n_gas + vm);
-            double dx = cm[0] - vc[0], dy = cm[1] - vc[1], dz = cm[2] - vc[2];
+            double dx = cx0 - __ldcg(vc), dy = cx1 - __ldcg(vc + 1), dz = cx2 - __ldcg(vc + 2);
             if ((dx * dx + dy * dy + dz * dz) < P->ml2) a->gvl[P->gvl_off + bgv + w++] = (unsigned short)q;
           }
       } else {
@@ -1930,8 +1945,9 @@ __device__ int vapor_entries(Ctx& x, int nreb) {
       }
       for (int u = threadIdx.x; u < G * ag && !clash; u += blockDim.x) {
         const double* gp = a->slab_x + 3 * ((size_t)P->slab_off + (size_t)par * P->slab_cap * ag + u);
+        const double g0 = __ldcg(gp), g1 = __ldcg(gp + 1), g2 = __ldcg(gp + 2);  /* moved this step by any CTA */
         for (int k = 0; k < av; k++) {
-          double dx = x.trial[3 * k] - gp[0], dy = x.trial[3 * k + 1] - gp[1], dz = x.trial[3 * k + 2] - gp[2];
+          double dx = x.trial[3 * k] - g0, dy = x.trial[3 * k + 1] - g1, dz = x.trial[3 * k + 2] - g2;
           if (dx * dx + dy * dy + dz * dz < d2min) clash = true;
         }
       }
@@ -2113,8 +2129,10 @@ __device__ void make_pair(Ctx& x, cg::cluster_group& cl) {
           for (int at = 0; at < ag; at++) {
             size_t go = gatom(P, par, os, at);
             for (int k = 0; k < 3; k++) {
-              X[3 * at + k] = a->slab_x[3 * go + k];
-              V[3 * at + k] = a->slab_v[3 * go + k];
+              /* the old slab slot may belong to another CTA, which moved
+               * it this step: from L2 */
+              X[3 * at + k] = __ldcg(a->slab_x + 3 * go + k);
+              V[3 * at + k] = __ldcg(a->slab_v + 3 * go + k);
             }
           }
         } else {

@@ -11,7 +11,7 @@ import pytest
 
 from md_nucleation_b200 import abi
 from tests import systems
-from tests.gpu_helpers import compare_states, force_ok, forces_of, need_gpu, rel_rms
+from tests.gpu_helpers import FORCE_ATOL, compare_states, force_ok, forces_of, need_gpu, rel_rms
 
 pytestmark = pytest.mark.gpu
 
@@ -74,8 +74,12 @@ def test_gg_fp64_pair_mode_forces(eng, oracle_libs, name):
     e.upload(0, st)
     e.compute_forces(abi.I_GG)
     o.compute_forces(abi.I_GG)
-    err = rel_rms(forces_of(e.state(0), spec), forces_of(o.get_state(), spec))
-    assert err <= 1e-9, f"relative RMS force error {err:.2e}"
+    fe, fo = forces_of(e.state(0), spec), forces_of(o.get_state(), spec)
+    err = rel_rms(fe, fo)
+    # helium's gas-gas forces are small: a few 2^-40 kcal/mol/A fixed-point
+    # quanta per atom then exceed 1e-9 of them
+    rms = np.sqrt(np.mean((fe - fo) ** 2))
+    assert err <= 1e-9 or rms <= FORCE_ATOL, f"relative RMS force error {err:.2e} (RMS {rms:.2e})"
 
 
 @pytest.mark.parametrize("name", NAMES)
