@@ -1214,9 +1214,8 @@ __device__ void gas_gg_pass(Ctx& x, cg::cluster_group& cl, bool eflag, bool fres
 
 /* LJ force of one (gas atom, core atom j) pair as 64-bit fixed point, the
  * force on the gas atom (PotentialGasIon / PotentialVaporGas: no Coulomb,
- * no taper weight).  The near pass adds it to the gas atom, the gather pass
- * subtracts it from core atom j: one expression, so the two sides cancel
- * exactly. */
+ * no taper weight); the near pass adds it to the gas atom and its negative
+ * to the core atom's sums. */
 template <bool FP64>
 __device__ __forceinline__ void gas_core_pair(const Ctx& x, const double* Xa, float3 ga, int ta, int j,
                                               long long* f) {
@@ -1235,63 +1234,6 @@ __device__ __forceinline__ void gas_core_pair(const Ctx& x, const double* Xa, fl
     const float fp = lj_coul(r2, x.c.ljA[ta * nt + tj], x.c.ljB[ta * nt + tj], 0.0f, false, &ee);
     f[0] = fixf(fp * dx); f[1] = fixf(fp * dy); f[2] = fixf(fp * dz);
   }
-}
-
-/* The reactions of the near gas molecules on the core, gathered: one warp
- * per row of the transposed lists (an ion atom, or a vapor molecule and each
- * of its first nj atoms), its lanes over the row's gas molecules, the sum
- * reduced across the warp and added to the core sums once.  The rows are
- * spread over the cluster's warps.  The gas positions (moved this step) and
- * the rows (built at the last rebuild) were written by any CTA of the
- * cluster, so they are read from L2 (__ldcg): this SM's L1 may still hold
- * the lines as it read them before. */
-template <int AG, bool FP64>
-__device__ void core_gather_t(Ctx& x) {
-  const RepParams* P = x.P;
-  const KArgs* a = x.a;
-  const int ni = P->n_ion, av = P->a_v, par = x.D->parity;
-  const int ne = ni + x.D->n_vap_in;
-  const bool gi = term_on(x, MDN_I_GI), gv = term_on(x, MDN_I_GV);
-  const int nj = (P->quirks & MDN_Q_GV_GAS_COUNT) ? min(AG, av) : av;
-  const int* tst = a->tr_start + P->tr_eoff;
-  const int* ent = a->tr + P->tr_off;
-  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  int gtype[AG];
-#pragma unroll
-  for (int at = 0; at < AG; at++) gtype[at] = x.ib[P->o_gas_type + at];
-  const double* com = x.D->ion_com;
-  for (int row = x.rank * nw + (int)(threadIdx.x >> 5); row < ne; row += x.C * nw) {
-    const bool ion_row = row < ni;
-    if (ion_row ? !gi : !gv) continue;
-    const int r0 = __ldcg(tst + row), rn = __ldcg(tst + row + 1) - r0;
-    const int nb = ion_row ? 1 : nj;
-    for (int b = 0; b < nb; b++) {
-      const int j = ion_row ? row : ni + (row - ni) * av + b;
-      long long R[3] = {0, 0, 0};
-      for (int q = lane; q < rn; q += 32) {
-        const int s = __ldcg(ent + r0 + q);
-#pragma unroll
-        for (int at = 0; at < AG; at++) {
-          const size_t g = gatom(P, par, s, at);
-          const double X[3] = {__ldcg(a->slab_x + 3 * g), __ldcg(a->slab_x + 3 * g + 1),
-                               __ldcg(a->slab_x + 3 * g + 2)};
-          const float3 gp = make_float3((float)(X[0] - com[0]), (float)(X[1] - com[1]), (float)(X[2] - com[2]));
-          long long f[3];
-          gas_core_pair<FP64>(x, X, gp, gtype[at], j, f);
-          R[0] -= f[0]; R[1] -= f[1]; R[2] -= f[2];
-        }
-      }
-      R[0] = warp_sum_ll(R[0]);
-      R[1] = warp_sum_ll(R[1]);
-      R[2] = warp_sum_ll(R[2]);
-      if (lane == 0 && (R[0] | R[1] | R[2])) acc_add(x, j, R);
-    }
-  }
-}
-
-__device__ void core_gather(Ctx& x) {
-  if (x.P->a_g == 1) core_gather_t<1, kFP64Pairs>(x);
-  else core_gather_t<2, kFP64Pairs>(x);
 }
 
 /* near molecules (those with a gas-ion or gas-vapor list entry): one thread
@@ -1353,14 +1295,17 @@ __device__ void gas_near_pass_t(Ctx& x, bool eflag, bool kick) {
       for (int q = 0; q < cnt; q++) {
         const int j = a->gil[P->gil_off + start + q];
         const int tj = x.c.type[j];
+        long long R[3] = {0, 0, 0};
         for (int at = 0; at < ag; at++) {
           long long f[3];
           gas_core_pair<FP64>(x, X + 3 * at, gp[at], gtype[at], j, f);
           F[at][0] += f[0]; F[at][1] += f[1]; F[at][2] += f[2];
+          R[0] -= f[0]; R[1] -= f[1]; R[2] -= f[2];
           if (eflag)
             egi += efixd(lj_coul_energy(r2d(X + 3 * at, x.c.x + 3 * j), x.db[P->d_ljA + gtype[at] * nt + tj],
                                         x.db[P->d_ljB + gtype[at] * nt + tj], 0.0));
         }
+        acc_add(x, j, R);
       }
     }
     if (gv) {
@@ -1370,14 +1315,17 @@ __device__ void gas_near_pass_t(Ctx& x, bool eflag, bool kick) {
         for (int b = 0; b < nj; b++) {
           const int j = ni + vs * av + b;
           const int tj = x.c.type[j];
+          long long R[3] = {0, 0, 0};
           for (int at = 0; at < ag; at++) {
             long long f[3];
             gas_core_pair<FP64>(x, X + 3 * at, gp[at], gtype[at], j, f);
             F[at][0] += f[0]; F[at][1] += f[1]; F[at][2] += f[2];
+            R[0] -= f[0]; R[1] -= f[1]; R[2] -= f[2];
             if (eflag)
               egv += efixd(lj_coul_energy(r2d(X + 3 * at, x.c.x + 3 * j), x.db[P->d_ljA + gtype[at] * nt + tj],
                                           x.db[P->d_ljB + gtype[at] * nt + tj], 0.0));
           }
+          acc_add(x, j, R);
         }
       }
     }
@@ -1462,7 +1410,6 @@ __device__ void core_reduce(Ctx& x, cg::cluster_group& cl) {
 __device__ void forces_and_kick(Ctx& x, cg::cluster_group& cl, bool eflag, bool kick) {
   prof_start(x);
   gas_near_pass(x, eflag, kick);
-  core_gather(x);
   __syncthreads();
   prof_end(x, MDN_PROF_NEAR);
   prof_start(x);
@@ -1734,61 +1681,6 @@ __device__ void relist_gg(Ctx& x, cg::cluster_group& cl) {
   cl.sync();
 }
 
-/* The gas-ion and gas-vapor lists by core partner: row j (ion atom) or
- * n_ion + q (vapor slab slot) holds the slab slots of the near gas molecules
- * that list it.  Counts per row, a prefix over the rows, then each molecule
- * takes a place in each of its partners' rows; the order inside a row does
- * not matter, since the reactions gathered from it are integer sums. */
-__device__ void transpose_lists(Ctx& x, cg::cluster_group& cl, int lo, int hi) {
-  const RepParams* P = x.P;
-  const KArgs* a = x.a;
-  const int par = x.D->parity, ni = P->n_ion, ne = ni + x.D->n_vap_in;
-  int* tst = a->tr_start + P->tr_eoff;
-  int* cur = a->tr_cur + P->tr_eoff;
-  int* ent = a->tr + P->tr_off;
-  int* sc = x.iscr;
-  if (x.rank == 0)
-    for (int e = threadIdx.x; e <= ne; e += blockDim.x) cur[e] = 0;
-  __threadfence();
-  cl.sync();
-  for (int pass = 0; pass < 2; pass++) {
-    for (int s = lo + (int)threadIdx.x; s < hi; s += blockDim.x) {
-      const size_t ms = gmol(P, par, s);
-      const int ng = a->gil_n[ms], nv = a->gvl_n[ms];
-      if (!(ng | nv)) continue;
-      const unsigned short* gl = a->gil + P->gil_off + a->near_gi[ms];
-      const unsigned short* vl = a->gvl + P->gvl_off + a->near_gv[ms];
-      for (int q = 0; q < ng + nv; q++) {
-        const int row = q < ng ? (int)gl[q] : ni + (int)vl[q - ng];
-        const int at = atomicAdd(&cur[row], 1);
-        if (pass) ent[at] = s;
-      }
-    }
-    __threadfence();
-    cl.sync();
-    if (pass == 0) {
-      /* counts -> row starts (rank 0), which the fill pass advances */
-      if (x.rank == 0) {
-        int run = 0;
-        for (int e0 = 0; e0 < ne; e0 += blockDim.x) {
-          const int e = e0 + threadIdx.x;
-          const int c = e < ne ? __ldcg(cur + e) : 0;
-          int t;
-          const int off = block_exscan(c, sc, &t);
-          if (e < ne) {
-            tst[e] = run + off;
-            cur[e] = run + off;
-          }
-          run += t;
-        }
-        if (threadIdx.x == 0) tst[ne] = run;
-      }
-      __threadfence();
-      cl.sync();
-    }
-  }
-}
-
 /* pair lists of the gas slab (current parity) from the centres: gas-ion
  * (PotentialGasIon::makePair) and gas-vapor (PotentialVaporGas::makePair) */
 __device__ void relist(Ctx& x, cg::cluster_group& cl) {
@@ -1909,7 +1801,6 @@ __device__ void relist(Ctx& x, cg::cluster_group& cl) {
   }
   __threadfence();
   cl.sync();
-  transpose_lists(x, cl, lo, hi);
   if (kGG && P->ggl_cap > 0 && (P->interactions & MDN_I_GG)) relist_gg(x, cl);
 }
 

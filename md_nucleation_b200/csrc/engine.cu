@@ -126,7 +126,6 @@ struct mdn_handle {
   int *near_gi = nullptr, *near_gv = nullptr;
   unsigned short *gil_n = nullptr, *gvl_n = nullptr, *gil = nullptr, *gvl = nullptr;
   int *ggl_start = nullptr, *ggl_n = nullptr, *ggl = nullptr, *slab_ins = nullptr;
-  int *tr_start = nullptr, *tr_cur = nullptr, *tr = nullptr;
   double* slab_fgg = nullptr;
   long long* energy = nullptr;
   DevEvent* events = nullptr;
@@ -153,7 +152,7 @@ struct mdn_handle {
   bool prof_on = false;
   /* sizes */
   size_t n_ion_tot = 0, n_mol_tot = 0, n_slab_atoms = 0, n_slab_mols = 0, n_vslab_atoms = 0,
-         n_vslab_mols = 0, n_near = 0, n_gil = 0, n_gvl = 0, n_ggl = 0, n_tr = 0, n_tre = 0;
+         n_vslab_mols = 0, n_near = 0, n_gil = 0, n_gvl = 0, n_ggl = 0;
   double last_ms = 0;
   long long last_launches = 0;
   /* snapshot staging */
@@ -173,7 +172,7 @@ void free_all(mdn_handle* h) {
                   h->gvl_n, h->gil, h->gvl, h->energy, h->events, h->n_events, h->status, h->job_order,
                   h->job_counter, h->snap_off, h->snap_type, h->snap_x, h->snap_v, h->d_ctl_mode,
                   h->d_ctl_T, h->d_prof, h->job_order2, h->job_counter2, h->ggl_start, h->ggl_n, h->ggl,
-                  h->slab_fgg, h->slab_ins, h->tr_start, h->tr_cur, h->tr};
+                  h->slab_fgg, h->slab_ins};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->ev0) cudaEventDestroy(h->ev0);
@@ -274,7 +273,6 @@ long long launch(mdn_handle* h, int mode, long long n_steps, int energy_mode, un
   a.gil_n = h->gil_n; a.gvl_n = h->gvl_n; a.gil = h->gil; a.gvl = h->gvl;
   a.ggl_start = h->ggl_start; a.ggl_n = h->ggl_n; a.ggl = h->ggl;
   a.slab_fgg = h->slab_fgg; a.slab_ins = h->slab_ins;
-  a.tr_start = h->tr_start; a.tr_cur = h->tr_cur; a.tr = h->tr;
   a.energy = h->energy;
   a.events = h->events; a.n_events = h->n_events; a.ev_cap = h->ev_cap;
   a.status = h->status;
@@ -401,7 +399,7 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
   h->P.resize(R);
   h->D0.resize(R);
   size_t ion_tot = 0, mol_tot = 0, slab_atoms = 0, slab_mols = 0, vslab_atoms = 0, vslab_mols = 0, near_tot = 0,
-         gil_tot = 0, gvl_tot = 0, ggl_tot = 0, tr_tot = 0, tre_tot = 0;
+         gil_tot = 0, gvl_tot = 0, ggl_tot = 0;
   for (int r = 0; r < R; r++) {
     const mdn_replica_desc& d = descs[r];
     RepParams& P = h->P[r];
@@ -640,10 +638,6 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
     gvl_tot += P.gvl_cap;
     P.ggl_off = (long long)ggl_tot;
     ggl_tot += P.ggl_cap;
-    P.tr_off = (long long)tr_tot;
-    tr_tot += (size_t)P.gil_cap + P.gvl_cap;
-    P.tr_eoff = (long long)tre_tot;
-    tre_tot += (size_t)d.ion.n_atoms + P.vcap + 1;
     P.work = eg * P.a_g + 0.05 * pow(d.ion.n_atoms + P.vcap * P.a_v * 0.5, 2) + near_est * d.ion.n_atoms;
 
     h->nt_cap = std::max(h->nt_cap, nt);
@@ -679,8 +673,6 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
   h->n_gil = gil_tot;
   h->n_gvl = gvl_tot;
   h->n_ggl = ggl_tot;
-  h->n_tr = tr_tot;
-  h->n_tre = tre_tot;
 
   /* job order: largest estimated work first */
   h->order.resize(R);
@@ -737,9 +729,6 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
   ALLOC(h->gvl_n, slab_mols);
   ALLOC(h->gil, gil_tot);
   ALLOC(h->gvl, gvl_tot);
-  ALLOC(h->tr_start, tre_tot);
-  ALLOC(h->tr_cur, tre_tot);
-  ALLOC(h->tr, tr_tot);
   if (ggl_tot > 0) {
     ALLOC(h->ggl_start, slab_mols);
     ALLOC(h->ggl_n, slab_mols);
@@ -788,7 +777,6 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
   ck(cudaMemset(h->status, 0, sizeof(int) * R), "status");
   ck(cudaMemset(h->near_gi, 0xff, sizeof(int) * slab_mols), "near_gi");
   if (h->slab_ins) ck(cudaMemset(h->slab_ins, 0xff, sizeof(int) * slab_mols), "slab_ins");
-  ck(cudaMemset(h->tr_start, 0, sizeof(int) * tre_tot), "tr_start");
   if (h->ggl_n) ck(cudaMemset(h->ggl_n, 0, sizeof(int) * slab_mols), "ggl_n");
   h->ctl_mode.resize(R);
   h->ctl_T.resize(R);

@@ -84,7 +84,6 @@ typedef struct RepParams {
   unsigned key0, key1;
   /* pool offsets (elements) */
   long long ion_off, mol_off, slab_off, vslab_off, near_off, gil_off, gvl_off, ggl_off;
-  long long tr_off, tr_eoff;      /* entries / per-partner rows of the transposed lists */
   long long slab_moff, vslab_moff; /* molecule offsets of the two slabs */
   long long iblob_off, dblob_off;
   double work;                   /* cost estimate for the job order */
@@ -130,10 +129,6 @@ typedef struct KArgs {
    * of each atom; the rebuild number that inserted the molecule (its taper
    * weights are 0 on the step of that rebuild); all NULL without gg */
   int *ggl_start, *ggl_n, *ggl;
-  /* the gas-ion and gas-vapor lists by core partner (ion atom j, or vapor
-   * slab slot q as row n_ion + q): the near gas molecules of each partner,
-   * so that a warp gathers the partner's whole reaction without atomics */
-  int *tr_start, *tr_cur, *tr;
   double* slab_fgg;
   int* slab_ins;
   long long* energy;       /* 8 per replica, fixed point                       */
