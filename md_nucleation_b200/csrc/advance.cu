@@ -234,6 +234,84 @@ __device__ __forceinline__ double shake_res_c(const double* Xi, const double* Xj
   return dr * dr;
 }
 
+/* Newton's method on one group of at most three constraints that share
+ * atoms (M-SHAKE).  The positions move along the constraints' reference
+ * bond vectors r_k exactly as in the sweeps (x_i += l_k r_k / m_i,
+ * x_j -= l_k r_k / m_j), and the l_k solve |s_k|^2 = d_k^2 for the whole
+ * group at once, so the result is the sweeps' fixed point; the equations
+ * are quadratic in l, and a handful of steps reach it where the sweeps of a
+ * rigid water take dozens.  For one constraint a step is the sweep's own
+ * update.  ks: the group's constraint indices (n of them); ct: the
+ * constraint table (d^2, 1/m_i, 1/m_j).  Returns true once every
+ * (|s_k|^2 - d_k^2)^2 <= 1e-20 A^4, the sweeps' criterion; false after 50
+ * steps or a singular system, and the caller sweeps from there. */
+__device__ bool shake_group(double* X, const double* R, const int* rig, const double* ct, const int* ks, int n) {
+  int I[3], J[3];
+  double r[3][3], d2[3], ci[3], cj[3], w[3][3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const int c = ks[k < n ? k : 0];
+    I[k] = rig[3 * c];
+    J[k] = rig[3 * c + 1];
+    d2[k] = ct[3 * c];
+    ci[k] = ct[3 * c + 1];
+    cj[k] = ct[3 * c + 2];
+#pragma unroll
+    for (int q = 0; q < 3; q++) r[k][q] = R[3 * I[k] + q] - R[3 * J[k] + q];
+  }
+  /* d s_k / d l_l = w_kl r_l; rows and columns past n: the identity */
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+#pragma unroll
+    for (int l = 0; l < 3; l++) {
+      const double ai = I[k] == I[l] ? ci[l] : (I[k] == J[l] ? -cj[l] : 0.0);
+      const double aj = J[k] == I[l] ? ci[l] : (J[k] == J[l] ? -cj[l] : 0.0);
+      w[k][l] = (k < n && l < n) ? ai - aj : 0.0;
+    }
+  for (int it = 0; it < 50; it++) {
+    double s[3][3], f[3];
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+#pragma unroll
+      for (int q = 0; q < 3; q++) s[k][q] = X[3 * I[k] + q] - X[3 * J[k] + q];
+      const double dr = s[k][0] * s[k][0] + s[k][1] * s[k][1] + s[k][2] * s[k][2] - d2[k];
+      f[k] = k < n ? dr : 0.0;
+      if (k < n && !(dr * dr <= 1e-20)) ok = false;
+    }
+    if (ok) return true;
+    double A[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+      for (int l = 0; l < 3; l++)
+        A[k][l] = (k < n && l < n) ? 2.0 * (s[k][0] * r[l][0] + s[k][1] * r[l][1] + s[k][2] * r[l][2]) * w[k][l]
+                                   : (k == l ? 1.0 : 0.0);
+    /* A d = -f by Cramer's rule */
+    const double c00 = A[1][1] * A[2][2] - A[1][2] * A[2][1];
+    const double c01 = A[1][0] * A[2][2] - A[1][2] * A[2][0];
+    const double c02 = A[1][0] * A[2][1] - A[1][1] * A[2][0];
+    const double det = A[0][0] * c00 - A[0][1] * c01 + A[0][2] * c02;
+    if (!(fabs(det) > 1e-300)) return false;
+    const double inv = 1.0 / det;
+    const double b0 = -f[0], b1 = -f[1], b2 = -f[2];
+    const double D0 = (b0 * c00 - A[0][1] * (b1 * A[2][2] - A[1][2] * b2) + A[0][2] * (b1 * A[2][1] - A[1][1] * b2)) * inv;
+    const double D1 = (A[0][0] * (b1 * A[2][2] - A[1][2] * b2) - b0 * c01 + A[0][2] * (A[1][0] * b2 - b1 * A[2][0])) * inv;
+    const double D2 = (A[0][0] * (A[1][1] * b2 - b1 * A[2][1]) - A[0][1] * (A[1][0] * b2 - b1 * A[2][0]) + b0 * c02) * inv;
+    const double Dl[3] = {D0, D1, D2};
+#pragma unroll
+    for (int l = 0; l < 3; l++) {
+      if (l >= n) break;
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        X[3 * I[l] + q] += Dl[l] * ci[l] * r[l][q];
+        X[3 * J[l] + q] -= Dl[l] * cj[l] * r[l][q];
+      }
+    }
+  }
+  return false;
+}
+
 template <int AG>
 __device__ void gas_integrate_t(Ctx& x, bool fused, bool eflag, int tid, int nthr);
 
@@ -275,8 +353,20 @@ __device__ void core_drift_shake(Ctx& x, bool fused, bool eflag) {
      * after a sweep */
     const int* rig = x.ib + P->o_ion_rigid;
     const int* col = x.ib + P->o_ion_color;
+    /* the ion's groups (an atom and its constrained hydrogens) share no
+     * atom: the lanes solve them independently */
+    bool done = false;
+    if (P->n_ion_groups > 0) {
+      const int* grp = x.ib + P->o_ion_grp;
+      const int* gst = x.ib + P->o_ion_gstart;
+      bool ok = true;
+      for (int g = lane; g < P->n_ion_groups; g += 32)
+        ok = shake_group(x.c.x, xold, rig, x.db + P->d_ion_cons, grp + gst[g], gst[g + 1] - gst[g]) && ok;
+      done = __all_sync(0xffffffffu, ok);
+      __syncwarp();
+    }
     int sweeps = 0;
-    for (;;) {
+    for (; !done;) {
       for (int c = 0; c < P->n_ion_colors; c++) {
         for (int k = lane; k < P->n_ion_rigid; k += 32) {
           if (col[k] != c) continue;
@@ -314,6 +404,13 @@ __device__ void core_drift_shake(Ctx& x, bool fused, bool eflag) {
       double* X = x.c.x + 3 * base;
       const double* R = xold + 3 * base;
       bool conv = false;
+      if (P->n_vap_groups > 0) {
+        const int* grp = x.ib + P->o_vap_grp;
+        const int* gst = x.ib + P->o_vap_gstart;
+        conv = true;
+        for (int g = 0; g < P->n_vap_groups; g++)
+          conv = shake_group(X, R, rig, ct, grp + gst[g], gst[g + 1] - gst[g]) && conv;
+      }
       for (int sweep = 0; sweep < MDN_SHAKE_MAX_SWEEPS && !conv; sweep++) {
         for (int c = 0; c < nco; c++)
           for (int k = 0; k < nr; k++) {

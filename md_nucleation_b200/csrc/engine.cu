@@ -19,6 +19,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <functional>
 #include <vector>
 
 #include "mdn.h"
@@ -93,6 +94,40 @@ int color_rigid(const int* rig, int n, std::vector<int>& color) {
     nc = std::max(nc, c + 1);
   }
   return nc;
+}
+
+/* the constraints' connected groups (constraints sharing an atom, joined
+ * transitively): order = constraint indices group by group, start = group
+ * starts (n_groups + 1).  Returns the number of groups, or 0 when a group
+ * holds more than 3 constraints (the kernel then sweeps). */
+int group_rigid(const int* rig, int n, std::vector<int>& order, std::vector<int>& start) {
+  order.clear();
+  start.clear();
+  if (n <= 0) return 0;
+  std::vector<int> parent(n);
+  for (int k = 0; k < n; k++) parent[k] = k;
+  std::function<int(int)> root = [&](int k) { return parent[k] == k ? k : parent[k] = root(parent[k]); };
+  for (int a = 0; a < n; a++)
+    for (int b = 0; b < a; b++)
+      if (rig[3 * a] == rig[3 * b] || rig[3 * a] == rig[3 * b + 1] || rig[3 * a + 1] == rig[3 * b] ||
+          rig[3 * a + 1] == rig[3 * b + 1])
+        parent[root(a)] = root(b);
+  std::vector<int> seen(n, 0);
+  for (int a = 0; a < n; a++) {
+    const int g = root(a);
+    if (seen[g]) continue;
+    seen[g] = 1;
+    start.push_back((int)order.size());
+    for (int k = 0; k < n; k++)
+      if (root(k) == g) order.push_back(k);
+    if ((int)order.size() - start.back() > 3) {
+      order.clear();
+      start.clear();
+      return 0;
+    }
+  }
+  start.push_back((int)order.size());
+  return (int)start.size() - 1;
 }
 
 }  // namespace
@@ -476,6 +511,12 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
     std::vector<int> col;
     P.n_ion_colors = color_rigid(d.ion.rigid, d.ion.n_rigid, col);
     P.o_ion_color = ipush(col.data(), (int)col.size());
+    {
+      std::vector<int> go, gs;
+      P.n_ion_groups = group_rigid(d.ion.rigid, d.ion.n_rigid, go, gs);
+      P.o_ion_grp = ipush(go.data(), (int)go.size());
+      P.o_ion_gstart = ipush(gs.data(), (int)gs.size());
+    }
     /* AMBER exclusions: 1-2 (bonds and rigid pairs), 1-3, 1-4 (compute_AMBER.cpp:256-278) */
     P.excl_words = (d.ion.n_atoms + 31) / 32;
     {
@@ -507,10 +548,16 @@ int mdn_create(const mdn_replica_desc* descs, int R, const mdn_options* opt_in, 
       P.o_vap_rigid = ipush(d.vapor.rigid, 3 * d.vapor.n_rigid);
       P.n_vap_colors = color_rigid(d.vapor.rigid, d.vapor.n_rigid, col);
       P.o_vap_color = ipush(col.data(), (int)col.size());
+      std::vector<int> go, gs;
+      P.n_vap_groups = group_rigid(d.vapor.rigid, d.vapor.n_rigid, go, gs);
+      P.o_vap_grp = ipush(go.data(), (int)go.size());
+      P.o_vap_gstart = ipush(gs.data(), (int)gs.size());
     } else {
       int zero = 0;
       P.o_vap_type = ipush(&zero, 1);
       P.o_vap_bonds = P.o_vap_angles = P.o_vap_dih = P.o_vap_rigid = P.o_vap_color = P.o_vap_type;
+      P.o_vap_grp = P.o_vap_gstart = P.o_vap_type;
+      P.n_vap_groups = 0;
     }
     P.o_dih_multi = ipush(d.dihedral_multi, d.n_dihedral_types);
 

@@ -70,6 +70,10 @@ typedef struct RepParams {
   int o_gas_type, o_gas_bonds, o_gas_rigid;
   int o_vap_type, o_vap_bonds, o_vap_angles, o_vap_dih, o_vap_rigid, o_vap_color;
   int o_dih_multi;
+  /* SHAKE constraints in groups of coupled ones (sharing atoms), at most 3
+   * per group, solved together (shake_group); 0 groups = colour sweeps */
+  int n_ion_groups, o_ion_grp, o_ion_gstart;
+  int n_vap_groups, o_vap_grp, o_vap_gstart;
   /* offsets inside the double blob */
   int d_bond, d_angle, d_dih, d_ljA, d_ljB, d_mass, d_c2;
   int d_ion_q, d_gas_x, d_gas_q, d_vap_x, d_vap_q;
