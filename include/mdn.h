@@ -53,7 +53,9 @@ extern "C" {
  * a molecule entering the domain is placed without an overlap test
  * (src/pairList/updateGasIn.cpp:51-98), as in the reference, so an entry on
  * top of another atom produces a huge force -- the reference carries on with
- * it, the engine carries on with each pair term saturated at 2^21 kcal/mol/A. */
+ * it, the engine carries on with its force terms saturated at 2^21
+ * kcal/mol/A (each gas pair term; for the core's own pairs, the sum of each
+ * 32 x 32 tile on an atom). */
 #define MDN_ST_FATAL (MDN_ST_SLAB_OVERFLOW | MDN_ST_CORE_OVERFLOW | MDN_ST_LIST_OVERFLOW | MDN_ST_NONFINITE)
 
 /* ---- Interactions keywords (src/initialization/setCondition.cpp:186-228) - */
@@ -420,19 +422,24 @@ int  mdn_set_launch(mdn_handle* h, int cluster_size, int threads, int steps_per_
 int  mdn_get_launch(mdn_handle* h, int* cluster_size, int* threads, int* steps_per_launch);
 /* Launch-shape tuner: advances every replica by n_steps at each cluster size
  * 1, 2, 4 and 8, timing each block with CUDA events, and keeps the fastest
- * size for later mdn_step calls (then tries the split launch below: up to 3
- * more blocks); *best (may be NULL) receives the cluster size.  The steps
- * are ordinary steps of the run: results do not depend on the launch shape.
- * A replica that fails during tuning is reported as mdn_step reports it.  */
+ * size for later mdn_step calls.  It then measures one block with the
+ * cycle accounting (mdn_profile) and orders the replicas by their measured
+ * cycles, slowest first, times one block in that order, and tries the split
+ * launch below (up to 8 more blocks); *best (may be NULL) receives the
+ * cluster size.  The steps are ordinary steps of the run: results do not
+ * depend on the launch shape or the order.  A replica that fails during
+ * tuning is reported as mdn_step reports it.  */
 int  mdn_tune_launch(mdn_handle* h, long long n_steps, int* best);
-/* Split step launch: the n_largest replicas with the most estimated work
- * run in a second launch, concurrent with the first on its own stream, on
+/* Split step launch: the n_largest replicas at the head of the job order
+ * (most estimated work, or most measured cycles once mdn_tune_launch has
+ * ordered them) run in a second launch, concurrent with the first on its own stream, on
  * clusters of cluster_size CTAs (one cluster each), and the other replicas
  * on the SMs left at the ordinary cluster size.  The launch of a batch is
  * as long as its largest replica on its cluster, so giving the few largest
  * more SMs shortens it.  n_largest = 0 turns it off.  mdn_tune_launch, when
- * no split is set, also times n_largest = 2, 4, 8 at twice the best cluster
- * size (n_steps each) and keeps a split that beats the best single launch.
+ * no split is set, also times n_largest = 2, 4, 8, 16 at two and four times
+ * the best cluster size (at most 8 CTAs; n_steps each) and keeps a split
+ * that beats the best single launch.
  * Results do not depend on the split.                                      */
 int  mdn_set_split(mdn_handle* h, int n_largest, int cluster_size);
 int  mdn_get_split(mdn_handle* h, int* n_largest, int* cluster_size);

@@ -39,6 +39,8 @@
  */
 #include <cooperative_groups.h>
 
+#include <type_traits>
+
 #include "device_util.cuh"
 #include "mdn_types.h"
 
@@ -764,8 +766,11 @@ __device__ __forceinline__ bool term_on(const Ctx& x, unsigned bit) {
  * distinct j (no bank conflicts), and it keeps the reaction on that j in a
  * register that moves one lane down after every step: after 32 steps lane l
  * holds the whole reaction on j = 32 jb + l.  Diagonal tiles take steps
- * 1..15 and half of step 16.  Both sides reach the core sums once per tile
- * as 64-bit integers, so the result does not depend on the launch shape. */
+ * 1..15 and half of step 16.  Each side is summed over the tile's steps in
+ * the pair precision, in that fixed order, and reaches the core sums once
+ * per tile as a 64-bit integer (one conversion per atom and tile instead of
+ * one per pair, 32-bit shuffles for the reactions), so the result does not
+ * depend on the launch shape. */
 template <bool FP64>
 __device__ void core_pairs_t(Ctx& x, bool eflag) {
   const RepParams* P = x.P;
@@ -802,7 +807,10 @@ __device__ void core_pairs_t(Ctx& x, bool eflag) {
       wid = weight_d(x, ii);
       qid = charge_d(x, ii);
     }
-    long long F0 = 0, F1 = 0, F2 = 0, R0 = 0, R1 = 0, R2 = 0;
+    /* the tile's sums in the pair arithmetic's own precision, in a fixed
+     * order (the tile's steps), turned into fixed point once per atom */
+    using Acc = typename std::conditional<FP64, double, float>::type;
+    Acc F0 = 0, F1 = 0, F2 = 0, R0 = 0, R1 = 0, R2 = 0;
     for (int s = 0; s < 32; s++) {
       const int j = jb * 32 + ((lane + s) & 31);
       bool take = act && j < nc;
@@ -846,7 +854,7 @@ __device__ void core_pairs_t(Ctx& x, bool eflag) {
           }
         }
         if (any) {
-          long long fx, fy, fz;
+          Acc fx, fy, fz;
           if constexpr (FP64) {
             /* the same terms in FP64 from the FP64 positions and tables */
             const double ex = xd[0] - x.c.x[3 * j], ey = xd[1] - x.c.x[3 * j + 1], ez = xd[2] - x.c.x[3 * j + 2];
@@ -861,13 +869,13 @@ __device__ void core_pairs_t(Ctx& x, bool eflag) {
             } else {
               fd = lj_coul_d(R2d, Ad, Bd, qq, true) * (wid * weight_d(x, j));
             }
-            fx = fixd(fd * ex);
-            fy = fixd(fd * ey);
-            fz = fixd(fd * ez);
+            fx = fd * ex;
+            fy = fd * ey;
+            fz = fd * ez;
           } else {
-            fx = fixf(fp * dx);
-            fy = fixf(fp * dy);
-            fz = fixf(fp * dz);
+            fx = fp * dx;
+            fy = fp * dy;
+            fz = fp * dz;
           }
           F0 += fx; F1 += fy; F2 += fz;
           R0 -= fx; R1 -= fy; R2 -= fz;
@@ -894,13 +902,17 @@ __device__ void core_pairs_t(Ctx& x, bool eflag) {
       R1 = __shfl_sync(0xffffffffu, R1, (lane + 1) & 31);
       R2 = __shfl_sync(0xffffffffu, R2, (lane + 1) & 31);
     }
-    if (act && (F0 | F1 | F2)) {
-      const long long F[3] = {F0, F1, F2};
+    auto fix = [](Acc v) -> long long {
+      if constexpr (FP64) return fixd(v);
+      else return fixf(v);
+    };
+    if (act && (F0 != 0 || F1 != 0 || F2 != 0)) {
+      const long long F[3] = {fix(F0), fix(F1), fix(F2)};
       acc_add(x, i, F);
     }
     const int jj = jb * 32 + lane;
-    if (jj < nc && (R0 | R1 | R2)) {
-      const long long Rv[3] = {R0, R1, R2};
+    if (jj < nc && (R0 != 0 || R1 != 0 || R2 != 0)) {
+      const long long Rv[3] = {fix(R0), fix(R1), fix(R2)};
       acc_add(x, jj, Rv);
     }
   }

@@ -1474,6 +1474,37 @@ int mdn_get_launch(mdn_handle* h, int* cluster_size, int* threads, int* steps_pe
   return MDN_OK;
 }
 
+/* One block of n_steps with the cycle accounting on; the job order becomes
+ * the replicas by measured cycles, largest first (the estimate from the
+ * sizes misses terms such as the gas-vapor lists of a dense gas around many
+ * vapor molecules).  The accounting is returned to the state it was in. */
+static int order_by_measured(mdn_handle* h, long long n_steps, int* status) {
+  const bool was_on = h->prof_on;
+  int rc = mdn_profile(h, 0, nullptr);
+  if (rc) return rc;
+  std::vector<long long> keep;
+  if (was_on) {
+    keep.resize((size_t)MDN_PROF_N * h->R);
+    if ((rc = mdn_profile(h, 1, keep.data()))) return rc;
+  }
+  CK(cudaMemset(h->d_prof, 0, sizeof(long long) * MDN_PROF_N * h->R));
+  h->prof_on = true;
+  rc = mdn_step(h, n_steps, 0);
+  if (rc == MDN_ERR_REPLICA) *status = rc;
+  else if (rc != MDN_OK) return rc;
+  std::vector<long long> prof((size_t)MDN_PROF_N * h->R);
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaMemcpy(prof.data(), h->d_prof, sizeof(long long) * prof.size(), cudaMemcpyDeviceToHost));
+  std::stable_sort(h->order.begin(), h->order.end(), [&](int a, int b) {
+    return prof[(size_t)a * MDN_PROF_N + MDN_PROF_TOTAL] > prof[(size_t)b * MDN_PROF_N + MDN_PROF_TOTAL];
+  });
+  /* the accounting as it was */
+  if (was_on) CK(cudaMemcpy(h->d_prof, keep.data(), sizeof(long long) * keep.size(), cudaMemcpyHostToDevice));
+  else CK(cudaMemset(h->d_prof, 0, sizeof(long long) * MDN_PROF_N * h->R));
+  h->prof_on = was_on;
+  return MDN_OK;
+}
+
 int mdn_tune_launch(mdn_handle* h, long long n_steps, int* best) {
   if (!h || n_steps <= 0) return fail(MDN_ERR_ARG, "bad arguments");
   int best_c = 0, status = MDN_OK;
@@ -1489,29 +1520,43 @@ int mdn_tune_launch(mdn_handle* h, long long n_steps, int* best) {
     }
   }
   h->opt.cluster_size = best_c;
-  /* then the largest replicas on clusters twice as large, beside the rest */
   const int save_n = h->split_n, save_c = h->split_cluster;
-  int best_n = 0;
-  if (save_n == 0 && 2 * best_c <= 8)
-    for (int k = 2; k <= 8 && k < h->R; k *= 2) {
-      if (k * 2 * best_c + best_c > h->num_sms) break;
-      h->split_n = k;
-      h->split_cluster = 2 * best_c;
-      int rc = mdn_step(h, n_steps, 0);
-      if (rc == MDN_ERR_REPLICA) status = rc;
-      else if (rc != MDN_OK) {
-        h->split_n = save_n;
-        h->split_cluster = save_c;
-        return rc;
+  if (save_n == 0) {
+    /* the replicas that bound the launch are the ones that take longest:
+     * order the jobs by measured cycles, then time the launch with that
+     * order */
+    int rc = order_by_measured(h, n_steps, &status);
+    if (rc) return rc;
+    rc = mdn_step(h, n_steps, 0);
+    if (rc == MDN_ERR_REPLICA) status = rc;
+    else if (rc != MDN_OK) return rc;
+    best_ms = h->last_ms;
+  }
+  /* then the k slowest replicas on larger clusters (2 or 4 times, at most 8
+   * CTAs), one each, in a concurrent launch beside the rest */
+  int best_n = 0, best_sc = 0;
+  if (save_n == 0)
+    for (int sc = 2 * best_c; sc <= 8; sc *= 2)
+      for (int k = 2; k <= 16 && k < h->R; k *= 2) {
+        if (k * sc + best_c > h->num_sms) break;
+        h->split_n = k;
+        h->split_cluster = sc;
+        int rc = mdn_step(h, n_steps, 0);
+        if (rc == MDN_ERR_REPLICA) status = rc;
+        else if (rc != MDN_OK) {
+          h->split_n = save_n;
+          h->split_cluster = save_c;
+          return rc;
+        }
+        if (h->last_ms < best_ms) {
+          best_n = k;
+          best_sc = sc;
+          best_ms = h->last_ms;
+        }
       }
-      if (h->last_ms < best_ms) {
-        best_n = k;
-        best_ms = h->last_ms;
-      }
-    }
   if (save_n == 0) {
     h->split_n = best_n;
-    h->split_cluster = best_n ? 2 * best_c : 0;
+    h->split_cluster = best_n ? best_sc : 0;
   }
   if (best) *best = best_c;
   return status;
