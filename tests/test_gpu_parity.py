@@ -183,14 +183,18 @@ def test_launch_shape_invariance(eng, threads, cluster):
 
 
 def test_tuned_launch_keeps_the_trajectory(eng):
-    """mdn_tune_launch runs ordinary steps at four cluster sizes: the state
-    equals that of the same number of steps at one fixed shape, bit for bit."""
+    """mdn_tune_launch runs ordinary steps at four cluster sizes, with the
+    cycle accounting on, in the measured job order and in split launches:
+    the state equals that of the same number of steps at one fixed shape,
+    bit for bit."""
     specs = [systems.make(n) for n in ("nacl_n2_meoh", "chain_he_water")]
     a = eng.Engine(specs, cluster_size=1)
     b = eng.Engine(specs)
-    a.step(4 * 20)
     best = b.tune_launch(20)
     assert best in (1, 2, 4, 8) and b.get_launch()[0] == best
+    steps = b.info(0).step
+    assert steps >= 4 * 20 and steps % 20 == 0
+    a.step(steps)
     for r in range(2):
         sa, sb = a.state(r), b.state(r)
         for name in ("ion_x", "ion_v", "mol_x", "mol_v", "gas_ax", "gas_av", "vap_ax", "vap_av"):
