@@ -114,7 +114,7 @@ __device__ __forceinline__ void set_status(const Ctx& x, int bit) {
 /* ------------------------------------------------------------------------- */
 /* core load / store                                                          */
 /* ------------------------------------------------------------------------- */
-__device__ void load_ion(Ctx& x) {
+__device__ __forceinline__ void load_ion(Ctx& x) {
   const RepParams* P = x.P;
   const KArgs* a = x.a;
   const int ni = P->n_ion;
@@ -132,7 +132,7 @@ __device__ void load_ion(Ctx& x) {
 }
 
 /* the vapor part of the core, from the vapor slab of the current parity */
-__device__ void load_vapor(Ctx& x) {
+__device__ __forceinline__ void load_vapor(Ctx& x) {
   const RepParams* P = x.P;
   const KArgs* a = x.a;
   const int ni = P->n_ion, av = P->a_v, nv = x.D->n_vap_in, par = x.D->parity;
@@ -152,7 +152,7 @@ __device__ void load_vapor(Ctx& x) {
   }
 }
 
-__device__ void store_core(Ctx& x) {
+__device__ __forceinline__ void store_core(Ctx& x) {
   const RepParams* P = x.P;
   const KArgs* a = x.a;
   if (x.rank != 0) return;
@@ -181,7 +181,7 @@ __device__ void store_core(Ctx& x) {
 /* ------------------------------------------------------------------------- */
 /* integration of the core                                                    */
 /* ------------------------------------------------------------------------- */
-__device__ void core_kick(Ctx& x) {
+__device__ __forceinline__ void core_kick(Ctx& x) {
   for (int i = threadIdx.x; i < x.n_core; i += blockDim.x) {
     double c2 = x.c.c2[x.c.type[i]];
     for (int k = 0; k < 3; k++) x.c.v[3 * i + k] += x.c.f[3 * i + k] * c2;
@@ -190,7 +190,7 @@ __device__ void core_kick(Ctx& x) {
 
 /* Observer::computeProps, ion part: Tion.  Warp 0, lane-strided sums then a
  * butterfly, so the result depends on the atom order only. */
-__device__ double ion_temperature(Ctx& x) {
+__device__ __forceinline__ double ion_temperature(Ctx& x) {
   const RepParams* P = x.P;
   if (threadIdx.x < 32) {
     double K = 0;
@@ -315,16 +315,16 @@ __device__ bool shake_group(double* X, const double* R, const int* rig, const do
 }
 
 template <int AG>
-__device__ void gas_integrate_t(Ctx& x, bool fused, bool eflag, int tid, int nthr);
+__device__ __forceinline__ void gas_integrate_t(Ctx& x, bool fused, bool eflag, int tid, int nthr);
 
-__device__ void gas_integrate(Ctx& x, bool fused, bool eflag, int tid, int nthr);
+__device__ __forceinline__ void gas_integrate(Ctx& x, bool fused, bool eflag, int tid, int nthr);
 
 /* Drift of the core, its constraints, and the gas integration of the step.
  * The constraints and the gas are independent (the gas pass touches only
  * the gas slab), so they run side by side: warp 0 sweeps the ion's
  * constraints, the next warps take one vapor molecule per thread, and the
  * remaining warps integrate the gas molecules. */
-__device__ void core_drift_shake(Ctx& x, bool fused, bool eflag) {
+__device__ __forceinline__ void core_drift_shake(Ctx& x, bool fused, bool eflag) {
   const RepParams* P = x.P;
   /* positions before the drift (the SHAKE reference vectors) live in the
    * 64-bit sum buffer: core_reduce overwrites it only after this step's
@@ -439,7 +439,7 @@ __device__ void core_drift_shake(Ctx& x, bool fused, bool eflag) {
 }
 
 /* ion centre: warp 0, lane-strided partial sums, butterfly, fixed order */
-__device__ void ion_centre(Ctx& x) {
+__device__ __forceinline__ void ion_centre(Ctx& x) {
   const RepParams* P = x.P;
   if (threadIdx.x < 32) {
     double s[6] = {0, 0, 0, 0, 0, 0};
@@ -461,7 +461,7 @@ __device__ void ion_centre(Ctx& x) {
 
 /* the ion centre in the reference's own order (sequential sum), used where a
  * threshold decision depends on it (the in/out classification) */
-__device__ void ion_centre_exact(Ctx& x) {
+__device__ __forceinline__ void ion_centre_exact(Ctx& x) {
   const RepParams* P = x.P;
   if (threadIdx.x == 0) {
     double s[6] = {0, 0, 0, 0, 0, 0};
@@ -495,7 +495,7 @@ __device__ __forceinline__ double taper(const RepParams* P, const double* com, c
  * of this step carries w < 0 and gets 0 for this step: MD::update_position
  * ran before the rebuild, while the molecule was still outside
  * (src/verlet.cpp:109-134), so the reference leaves its weights unset. */
-__device__ void core_weights_pos(Ctx& x, bool weights) {
+__device__ __forceinline__ void core_weights_pos(Ctx& x, bool weights) {
   const RepParams* P = x.P;
   const double* com = x.D->ion_com;
   for (int i = threadIdx.x; i < x.n_core; i += blockDim.x) {
@@ -772,7 +772,7 @@ __device__ __forceinline__ bool term_on(const Ctx& x, unsigned bit) {
  * one per pair, 32-bit shuffles for the reactions), so the result does not
  * depend on the launch shape. */
 template <bool FP64>
-__device__ void core_pairs_t(Ctx& x, bool eflag) {
+__device__ __forceinline__ void core_pairs_t(Ctx& x, bool eflag) {
   const RepParams* P = x.P;
   const int ni = P->n_ion, nc = x.n_core, nt = P->n_types;
   const bool amber = term_on(x, MDN_I_AMBER), bmh = term_on(x, MDN_I_BMH);
@@ -938,7 +938,7 @@ constexpr bool kFP64Pairs = true;
 constexpr bool kFP64Pairs = false;
 #endif
 
-__device__ void core_pairs(Ctx& x, bool eflag) { core_pairs_t<kFP64Pairs>(x, eflag); }
+__device__ __forceinline__ void core_pairs(Ctx& x, bool eflag) { core_pairs_t<kFP64Pairs>(x, eflag); }
 
 /* MDN_GG_TERMS selects the gas-gas term: compiled into its own kernels
  * (advance_gg.cu, advance_gg_fp64.cu), absent from the others */
@@ -948,7 +948,7 @@ constexpr bool kGG = true;
 constexpr bool kGG = false;
 #endif
 
-__device__ void core_bonded(Ctx& x, bool eflag) {
+__device__ __forceinline__ void core_bonded(Ctx& x, bool eflag) {
   const RepParams* P = x.P;
   const bool amber = term_on(x, MDN_I_AMBER);
   const bool vin = term_on(x, MDN_I_VAPOR_INTRA);
@@ -1086,7 +1086,7 @@ __device__ __forceinline__ int shake_gas2(const Ctx& x, double* X, const double*
  * the intramolecular force and second kick of the gas molecules; thread tid
  * of the nthr (whole warps) that take part */
 template <int AG>
-__device__ void gas_integrate_t(Ctx& x, bool fused, bool eflag, int tid, int nthr) {
+__device__ __forceinline__ void gas_integrate_t(Ctx& x, bool fused, bool eflag, int tid, int nthr) {
   const RepParams* P = x.P;
   const KArgs* a = x.a;
   constexpr int ag = AG;
@@ -1159,14 +1159,14 @@ __device__ void gas_integrate_t(Ctx& x, bool fused, bool eflag, int tid, int nth
   }
 }
 
-__device__ void gas_integrate(Ctx& x, bool fused, bool eflag, int tid, int nthr) {
+__device__ __forceinline__ void gas_integrate(Ctx& x, bool fused, bool eflag, int tid, int nthr) {
   if (x.P->a_g == 1) gas_integrate_t<1>(x, fused, eflag, tid, nthr);
   else gas_integrate_t<2>(x, fused, eflag, tid, nthr);
 }
 
 /* after a rebuild: intramolecular force and second kick of the far molecules */
 template <int AG>
-__device__ void gas_far_pass_t(Ctx& x, bool eflag, bool kick) {
+__device__ __forceinline__ void gas_far_pass_t(Ctx& x, bool eflag, bool kick) {
   const RepParams* P = x.P;
   const KArgs* a = x.a;
   constexpr int ag = AG;
@@ -1210,7 +1210,7 @@ __device__ void gas_far_pass_t(Ctx& x, bool eflag, bool kick) {
   }
 }
 
-__device__ void gas_far_pass(Ctx& x, bool eflag, bool kick) {
+__device__ __forceinline__ void gas_far_pass(Ctx& x, bool eflag, bool kick) {
   if (x.P->a_g == 1) gas_far_pass_t<1>(x, eflag, kick);
   else gas_far_pass_t<2>(x, eflag, kick);
 }
@@ -1228,7 +1228,7 @@ __device__ void gas_far_pass(Ctx& x, bool eflag, bool kick) {
  * MD::update_position sets them (src/verlet.cpp:109-134); molecules the
  * rebuild of this step inserted have weight 0 (`fresh`: this step rebuilt). */
 template <int AG, bool FP64>
-__device__ void gas_gg_pass_t(Ctx& x, bool eflag, bool fresh) {
+__device__ __forceinline__ void gas_gg_pass_t(Ctx& x, bool eflag, bool fresh) {
   const RepParams* P = x.P;
   const KArgs* a = x.a;
   const int par = x.D->parity, nt = P->n_types, nreb = x.D->n_rebuilds;
@@ -1310,7 +1310,7 @@ __device__ void gas_gg_pass_t(Ctx& x, bool eflag, bool fresh) {
 
 /* the gas-gas forces of this step, when gg LJ is on: every CTA of the
  * cluster must see the final gas positions first */
-__device__ void gas_gg_pass(Ctx& x, cg::cluster_group& cl, bool eflag, bool fresh) {
+__device__ __forceinline__ void gas_gg_pass(Ctx& x, cg::cluster_group& cl, bool eflag, bool fresh) {
   if constexpr (kGG) {
     if (!(term_on(x, MDN_I_GG) && x.P->ggl_cap > 0)) return;
     __threadfence();
@@ -1345,18 +1345,56 @@ __device__ __forceinline__ void gas_core_pair(const Ctx& x, const double* Xa, fl
   }
 }
 
-/* near molecules (those with a gas-ion or gas-vapor list entry): one thread
- * each, walking the molecule's lists (about one entry per molecule in the
- * batched workload, so a wider split leaves lanes idle); the molecule's own
- * force stays in registers, the reaction goes to the core sums by shared
- * 32-bit integer atomics on exact chunks (acc_add), so the result does not
- * depend on the order */
+/* One core partner j of a near gas molecule: the LJ pairs of its AG atoms
+ * with j, their forces added to F (64-bit fixed point), the reaction on j to
+ * the core sums (shared 32-bit atomics on exact chunks, acc_add), and with
+ * eflag the pair energy to e.  X holds the molecule's FP64 positions (used
+ * by the FP64 pairs and the energies), gp its FP32 positions relative to the
+ * ion centre. */
 template <int AG, bool FP64>
-__device__ void gas_near_pass_t(Ctx& x, bool eflag, bool kick) {
+__device__ __forceinline__ void near_partner(Ctx& x, const double* X, const float3* gp, const int* gtype, int j,
+                                             bool eflag, long long (*F)[3], long long& e) {
+  const RepParams* P = x.P;
+  const int nt = P->n_types, tj = x.c.type[j];
+  long long R[3] = {0, 0, 0};
+#pragma unroll
+  for (int at = 0; at < AG; at++) {
+    long long f[3];
+    gas_core_pair<FP64>(x, X + 3 * at, gp[at], gtype[at], j, f);
+    F[at][0] += f[0]; F[at][1] += f[1]; F[at][2] += f[2];
+    R[0] -= f[0]; R[1] -= f[1]; R[2] -= f[2];
+    if (eflag)
+      e += efixd(lj_coul_energy(r2d(X + 3 * at, x.c.x + 3 * j), x.db[P->d_ljA + gtype[at] * nt + tj],
+                                x.db[P->d_ljB + gtype[at] * nt + tj], 0.0));
+  }
+  acc_add(x, j, R);
+}
+
+/* A near molecule with more partners than this has them spread over a warp. */
+constexpr int kNearHeavy = 16;
+
+/* near molecules (those with a gas-ion or gas-vapor list entry).  Partner
+ * counts (gas-ion entries, plus gas-vapor entries times the vapor atoms each
+ * reaches) are uneven: the few dozen to few hundred molecules next to a
+ * large ion have 30-100 gas-ion entries, the thousands near vapor 1-13
+ * gas-vapor partners.  So, first, each warp takes 32 of the CTA's near
+ * molecules at a time and spreads the partners of those with more than
+ * kNearHeavy over its lanes, one molecule after another, their force summed
+ * by shuffles and parked, as 64-bit integers, in the molecule's slab force
+ * rows.  Then one thread per near molecule walks the other molecules'
+ * lists (the lanes of a warp run through their molecules independently, so
+ * uneven light walks even out over a lane's several molecules), takes the
+ * parked force of the heavy ones, and finishes each molecule: its force,
+ * the gas-gas and intramolecular terms and the second kick.  Each reaction
+ * goes to the core sums by shared 32-bit integer atomics on exact chunks
+ * (acc_add); all sums are integers, so neither the split nor the order
+ * changes the result. */
+template <int AG, bool FP64>
+__device__ __forceinline__ void gas_near_pass_t(Ctx& x, bool eflag, bool kick) {
   const RepParams* P = x.P;
   const KArgs* a = x.a;
   constexpr int ag = AG;
-  const int av = P->a_v, par = x.D->parity, nt = P->n_types, ni = P->n_ion;
+  const int av = P->a_v, par = x.D->parity, ni = P->n_ion;
   const bool gi = term_on(x, MDN_I_GI), gv = term_on(x, MDN_I_GV);
   const bool intra = term_on(x, MDN_I_GAS_INTRA) && P->n_gas_bonds > 0;
   const bool gg = kGG && term_on(x, MDN_I_GG) && P->ggl_cap > 0;
@@ -1384,6 +1422,58 @@ __device__ void gas_near_pass_t(Ctx& x, bool eflag, bool kick) {
   }
   const double* com = x.D->ion_com;
   long long egi = 0, egv = 0, eintra = 0;
+  /* heavy molecules, spread over a warp */
+  {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    for (int c0 = b0 + (int)(threadIdx.x & ~31u); c0 < b1; c0 += blockDim.x) {
+      const int e = c0 + lane;
+      int items = 0;
+      if (e < b1) {
+        const size_t ms = gmol(P, par, nl[e]);
+        items = (gi ? (int)a->gil_n[ms] : 0) + (gv ? (int)a->gvl_n[ms] * nj : 0);
+      }
+      for (unsigned heavy = __ballot_sync(FULL, items > kNearHeavy); heavy; heavy &= heavy - 1) {
+        const int so = nl[c0 + __ffs(heavy) - 1];
+        const size_t ms = gmol(P, par, so);
+        const int ngo = gi ? a->gil_n[ms] : 0, nvo = gv ? a->gvl_n[ms] : 0;
+        const int sgo = a->near_gi[ms], svo = a->near_gv[ms];
+        float3 gpo[AG];
+        double Xo[3 * AG];
+#pragma unroll
+        for (int at = 0; at < AG; at++) {
+          const size_t g = gatom(P, par, so, at);
+#pragma unroll
+          for (int k = 0; k < 3; k++) Xo[3 * at + k] = a->slab_x[3 * g + k];
+          gpo[at] = make_float3((float)(Xo[3 * at] - com[0]), (float)(Xo[3 * at + 1] - com[1]),
+                                (float)(Xo[3 * at + 2] - com[2]));
+        }
+        long long Fo[AG][3];
+#pragma unroll
+        for (int at = 0; at < AG; at++) Fo[at][0] = Fo[at][1] = Fo[at][2] = 0;
+        const int n_it = ngo + nvo * nj;
+        for (int it = lane; it < n_it; it += 32) {
+          if (it < ngo) {
+            near_partner<AG, FP64>(x, Xo, gpo, gtype, (int)a->gil[P->gil_off + sgo + it], eflag, Fo, egi);
+          } else {
+            const int t = it - ngo, ent = t / nj, b = t - ent * nj;
+            near_partner<AG, FP64>(x, Xo, gpo, gtype, ni + (int)a->gvl[P->gvl_off + svo + ent] * av + b, eflag,
+                                   Fo, egv);
+          }
+        }
+#pragma unroll
+        for (int at = 0; at < AG; at++) {
+          const size_t g = gatom(P, par, so, at);
+#pragma unroll
+          for (int k = 0; k < 3; k++) {
+            const long long v = warp_sum_ll(Fo[at][k]);
+            if (lane == 0) a->slab_f[3 * g + k] = __longlong_as_double(v);
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
   for (int e = b0 + (int)threadIdx.x; e < b1; e += blockDim.x) {
     const int s = nl[e];
     const size_t ms = gmol(P, par, s);
@@ -1399,50 +1489,25 @@ __device__ void gas_near_pass_t(Ctx& x, bool eflag, bool kick) {
     long long F[AG][3];
 #pragma unroll
     for (int at = 0; at < AG; at++) F[at][0] = F[at][1] = F[at][2] = 0;
-    if (gi) {
-      const int start = a->near_gi[ms], cnt = a->gil_n[ms];
-      for (int q = 0; q < cnt; q++) {
-        const int j = a->gil[P->gil_off + start + q];
-        const int tj = x.c.type[j];
-        long long R[3] = {0, 0, 0};
-        for (int at = 0; at < ag; at++) {
-          long long f[3];
-          gas_core_pair<FP64>(x, X + 3 * at, gp[at], gtype[at], j, f);
-          F[at][0] += f[0]; F[at][1] += f[1]; F[at][2] += f[2];
-          R[0] -= f[0]; R[1] -= f[1]; R[2] -= f[2];
-          if (eflag)
-            egi += efixd(lj_coul_energy(r2d(X + 3 * at, x.c.x + 3 * j), x.db[P->d_ljA + gtype[at] * nt + tj],
-                                        x.db[P->d_ljB + gtype[at] * nt + tj], 0.0));
-        }
-        acc_add(x, j, R);
-      }
-    }
-    if (gv) {
-      const int start = a->near_gv[ms], cnt = a->gvl_n[ms];
-      for (int ent = 0; ent < cnt; ent++) {
-        const int vs = a->gvl[P->gvl_off + start + ent];
-        for (int b = 0; b < nj; b++) {
-          const int j = ni + vs * av + b;
-          const int tj = x.c.type[j];
-          long long R[3] = {0, 0, 0};
-          for (int at = 0; at < ag; at++) {
-            long long f[3];
-            gas_core_pair<FP64>(x, X + 3 * at, gp[at], gtype[at], j, f);
-            F[at][0] += f[0]; F[at][1] += f[1]; F[at][2] += f[2];
-            R[0] -= f[0]; R[1] -= f[1]; R[2] -= f[2];
-            if (eflag)
-              egv += efixd(lj_coul_energy(r2d(X + 3 * at, x.c.x + 3 * j), x.db[P->d_ljA + gtype[at] * nt + tj],
-                                          x.db[P->d_ljB + gtype[at] * nt + tj], 0.0));
-          }
-          acc_add(x, j, R);
-        }
+    /* a heavy molecule's force was parked by its warp */
+    const int ngi = gi ? a->gil_n[ms] : 0, ngv = gv ? a->gvl_n[ms] : 0;
+    const bool heavy = ngi + ngv * nj > kNearHeavy;
+    {
+      const int sgi = a->near_gi[ms], sgv = a->near_gv[ms];
+      const int cgi = heavy ? 0 : ngi, cgv = heavy ? 0 : ngv;
+      for (int q = 0; q < cgi; q++)
+        near_partner<AG, FP64>(x, X, gp, gtype, (int)a->gil[P->gil_off + sgi + q], eflag, F, egi);
+      for (int ent = 0; ent < cgv; ent++) {
+        const int vs = a->gvl[P->gvl_off + sgv + ent];
+        for (int b = 0; b < nj; b++) near_partner<AG, FP64>(x, X, gp, gtype, ni + vs * av + b, eflag, F, egv);
       }
     }
     double Fd[3 * AG];
 #pragma unroll
     for (int at = 0; at < ag; at++)
       for (int k = 0; k < 3; k++) {
-        Fd[3 * at + k] = (double)F[at][k] * MDN_FIX_INV;
+        const long long v = heavy ? __double_as_longlong(a->slab_f[3 * gatom(P, par, s, at) + k]) : F[at][k];
+        Fd[3 * at + k] = (double)v * MDN_FIX_INV;
         if (!(fabs(Fd[3 * at + k]) < MDN_FIX_LIMIT)) set_status(x, MDN_ST_FIXED_OVERFLOW);
       }
     if (gg)
@@ -1472,13 +1537,13 @@ __device__ void gas_near_pass_t(Ctx& x, bool eflag, bool kick) {
   }
 }
 
-__device__ void gas_near_pass(Ctx& x, bool eflag, bool kick) {
+__device__ __forceinline__ void gas_near_pass(Ctx& x, bool eflag, bool kick) {
   if (x.P->a_g == 1) gas_near_pass_t<1, kFP64Pairs>(x, eflag, kick);
   else gas_near_pass_t<2, kFP64Pairs>(x, eflag, kick);
 }
 
 /* sum of the core partials over the cluster -> f (double), identical in every CTA */
-__device__ void core_reduce(Ctx& x, cg::cluster_group& cl) {
+__device__ __forceinline__ void core_reduce(Ctx& x, cg::cluster_group& cl) {
   const int n3 = 3 * x.n_core;
   long long* mine = x.c.acc;
   /* fold the chunk sums into this CTA's 64-bit sums (each thread its own
@@ -1516,7 +1581,7 @@ __device__ void core_reduce(Ctx& x, cg::cluster_group& cl) {
 }
 
 /* all forces of the step (after positions and lists are final) and the second kick */
-__device__ void forces_and_kick(Ctx& x, cg::cluster_group& cl, bool eflag, bool kick) {
+__device__ __forceinline__ void forces_and_kick(Ctx& x, cg::cluster_group& cl, bool eflag, bool kick) {
   prof_start(x);
   gas_near_pass(x, eflag, kick);
   __syncthreads();
@@ -1544,14 +1609,14 @@ __device__ void forces_and_kick(Ctx& x, cg::cluster_group& cl, bool eflag, bool 
 /* Philox word of insertion draw `t` (word 1 is the N2 spin) */
 __device__ __forceinline__ int insert_word(int t) { return t == 0 ? 0 : 1 + t; }
 
-__device__ void insert_vapor(const Ctx& x, int q, int n_rebuild, int t, double* X, double* V);
+__device__ __forceinline__ void insert_vapor(const Ctx& x, int q, int n_rebuild, int t, double* X, double* V);
 
 /* true when no atom of X[0..n) lies within MDN_INSERT_MIN_DIST of a core atom
  * (ion, vapor in the domain before this rebuild) or of a vapor molecule whose
  * entry this rebuild already accepted; with the gas-gas term on, nor of a gas
  * atom in the domain before this rebuild (gas molecules entering in the same
  * rebuild are not tested against each other) */
-__device__ bool insert_clear(const Ctx& x, const double* X, int n, int n_rebuild) {
+__device__ __forceinline__ bool insert_clear(const Ctx& x, const double* X, int n, int n_rebuild) {
   const double d2min = MDN_INSERT_MIN_DIST * MDN_INSERT_MIN_DIST;
   if (kGG && (x.P->interactions & MDN_I_GG)) {
     const RepParams* P = x.P;
@@ -1588,7 +1653,7 @@ __device__ bool insert_clear(const Ctx& x, const double* X, int n, int n_rebuild
   return true;
 }
 
-__device__ void insert_gas(const Ctx& x, int q, int n_rebuild, int t, double* X, double* V) {
+__device__ __forceinline__ void insert_gas(const Ctx& x, int q, int n_rebuild, int t, double* X, double* V) {
   const RepParams* P = x.P;
   const int ag = P->a_g, mi = 1 + q;
   const double* cx = x.a->mol_x + 3 * ((size_t)P->mol_off + mi);
@@ -1625,7 +1690,7 @@ __device__ void insert_gas(const Ctx& x, int q, int n_rebuild, int t, double* X,
   }
 }
 
-__device__ void insert_vapor(const Ctx& x, int q, int n_rebuild, int t, double* X, double* V) {
+__device__ __forceinline__ void insert_vapor(const Ctx& x, int q, int n_rebuild, int t, double* X, double* V) {
   const RepParams* P = x.P;
   const int av = P->a_v, mi = 1 + P->n_gas + q;
   const double* cx = x.a->mol_x + 3 * ((size_t)P->mol_off + mi);
@@ -1715,7 +1780,7 @@ __device__ __forceinline__ int classify_one(const Ctx& x, int mi, double sigma, 
 
 /* exchange one int per CTA across the cluster: returns the prefix before this
  * rank and the total */
-__device__ void cluster_prefix(Ctx& x, cg::cluster_group& cl, int* slot_in_smem, int mine, int* before,
+__device__ __forceinline__ void cluster_prefix(Ctx& x, cg::cluster_group& cl, int* slot_in_smem, int mine, int* before,
                                int* total) {
   if (threadIdx.x == 0) *slot_in_smem = mine;
   cl.sync();
@@ -1734,7 +1799,7 @@ __device__ void cluster_prefix(Ctx& x, cg::cluster_group& cl, int* slot_in_smem,
  * src/potential/GasGas.cpp:41-62, on the in-domain molecules it was meant
  * for): every other slab molecule whose centre lies within the list radius,
  * both directions, ascending slab slot, CSR by slab slot over the cluster */
-__device__ void relist_gg(Ctx& x, cg::cluster_group& cl) {
+__device__ __forceinline__ void relist_gg(Ctx& x, cg::cluster_group& cl) {
   const RepParams* P = x.P;
   const KArgs* a = x.a;
   const int par = x.D->parity, G = x.D->n_gas_in;
@@ -1792,7 +1857,7 @@ __device__ void relist_gg(Ctx& x, cg::cluster_group& cl) {
 
 /* pair lists of the gas slab (current parity) from the centres: gas-ion
  * (PotentialGasIon::makePair) and gas-vapor (PotentialVaporGas::makePair) */
-__device__ void relist(Ctx& x, cg::cluster_group& cl) {
+__device__ __forceinline__ void relist(Ctx& x, cg::cluster_group& cl) {
   const RepParams* P = x.P;
   const KArgs* a = x.a;
   const int par = x.D->parity, ni = P->n_ion, nv = x.D->n_vap_in;
@@ -1917,7 +1982,7 @@ __device__ void relist(Ctx& x, cg::cluster_group& cl) {
  * already in the domain and every in-domain gas atom (up to ~20,000), so the
  * whole block tests each candidate's draws.  Rank 0 only; returns the number
  * of entries that must wait. */
-__device__ int vapor_entries(Ctx& x, int nreb) {
+__device__ __forceinline__ int vapor_entries(Ctx& x, int nreb) {
   const RepParams* P = x.P;
   const KArgs* a = x.a;
   const int av = P->a_v, ag = P->a_g, par = x.D->parity, G = x.D->n_gas_in;
@@ -1974,7 +2039,7 @@ __device__ int vapor_entries(Ctx& x, int nreb) {
   return d;
 }
 
-__device__ void make_pair(Ctx& x, cg::cluster_group& cl) {
+__device__ __forceinline__ void make_pair(Ctx& x, cg::cluster_group& cl) {
   const RepParams* P = x.P;
   const KArgs* a = x.a;
   const int ag = P->a_g, av = P->a_v, par = x.D->parity, npar = par ^ 1;
@@ -2226,7 +2291,7 @@ __device__ void make_pair(Ctx& x, cg::cluster_group& cl) {
 }
 
 /* ------------------------------------------------------------------------- */
-__device__ void one_step(Ctx& x, cg::cluster_group& cl, bool eflag) {
+__device__ __forceinline__ void one_step(Ctx& x, cg::cluster_group& cl, bool eflag) {
   const RepParams* P = x.P;
   prof_start(x);
   core_kick(x);
