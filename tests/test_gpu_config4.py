@@ -52,3 +52,22 @@ def test_config4_trajectory(case):
     o.step(20)
     assert e.status()[0] == 0
     compare_states(e.state(0), o.get_state(), spec, xtol=1e-6, vtol=1e-7, what="config 4")
+
+
+def test_config4_pair_lists_match_oracle(case):
+    """The cell-binned list build on the largest core (the 500-atom chain and
+    the in-domain water) against the oracle's all-pairs rule for the same
+    state (GasIon.cpp:41-60, VaporGas.cpp:5-64): equal as sets."""
+    eng, spec, o = case
+    st = o.get_state()
+    o.set_state(st)
+    e = eng.Engine([spec])
+    e.upload(0, st)
+    n = 0
+    for kind in (0, 1):
+        got = {tuple(p) for p in e.pair_list(0, kind)}
+        want = {tuple(p) for p in o.pair_list(kind)}
+        assert got == want, kind
+        n += len(want)
+    assert n > 0
+    e.close()

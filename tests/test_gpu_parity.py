@@ -48,6 +48,32 @@ def test_initial_make_pair_matches_oracle(eng, oracle_libs, name, quirks):
         assert {tuple(p) for p in e.pair_list(0, kind)} == {tuple(p) for p in o.pair_list(kind)}
 
 
+def test_pair_lists_after_steps_match_oracle(eng, oracle_libs):
+    """The cell-binned list build against the oracle's all-pairs rule on two
+    replicas of the batched workload (a 69- and a 221-atom ion, dozens to a
+    hundred in-domain vapor molecules) after 300 steps: the state is loaded
+    into a fresh engine, whose upload rebuilds the lists, and into the oracle,
+    whose set_state does; the lists are equal as sets."""
+    from md_nucleation_b200 import generate
+    specs = [generate.config2_replica(r) for r in (24, 42)]
+    e = eng.Engine(specs, quirks=CHECKED)
+    e.step(300)
+    assert (e.status() & abi.ST_FATAL).sum() == 0
+    for r, spec in enumerate(specs):
+        S = e.state(r)
+        o = oracle_libs.OracleReplica(spec, quirks=CHECKED)
+        o.set_state(S)
+        f = eng.Engine([spec], quirks=CHECKED)
+        f.upload(0, S)
+        for kind in (0, 1):
+            got = {tuple(p) for p in f.pair_list(0, kind)}
+            want = {tuple(p) for p in o.pair_list(kind)}
+            assert got == want and len(want) > 0, (r, kind)
+        f.close()
+        o.close()
+    e.close()
+
+
 @pytest.mark.parametrize("name", NAMES)
 @pytest.mark.parametrize("term", [0, abi.I_GI, abi.I_VI, abi.I_VV, abi.I_GV, abi.I_AMBER, abi.I_BMH,
                                   abi.I_GAS_INTRA, abi.I_VAPOR_INTRA])
