@@ -423,11 +423,52 @@ __device__ void forces(const Sys& S, const Buf& B, const double* x, double* F) {
   __syncthreads();
 }
 
+/* The parameter derivatives of the pair loops, summed in registers: the
+ * pairs are sorted by kind and type pair, so a thread's run of pairs keeps
+ * one (eps, sigma) row for many pairs and adds its sums to the shared
+ * gradient when the row changes; the charge scale, which every charged pair
+ * touches, is summed over the warp first.  (Adding every pair's terms to the
+ * few shared rows directly serialised the pair loops on those addresses.) */
+__device__ __forceinline__ double warp_sum_dd(double v) {
+#pragma unroll
+  for (int m = 16; m >= 1; m >>= 1) v += __shfl_xor_sync(0xffffffffu, v, m);
+  return v;
+}
+
+struct ParamSums {
+  int p = -1;
+  double e = 0, s = 0, q = 0;
+  __device__ __forceinline__ void add_lj(double* sgrad, int row, double de, double ds) {
+    if (row != p) {
+      flush_lj(sgrad);
+      p = row;
+    }
+    e += de;
+    s += ds;
+  }
+  __device__ __forceinline__ void flush_lj(double* sgrad) {
+    if (p >= 0) {
+      atomicAdd(&sgrad[p], e);
+      atomicAdd(&sgrad[p + 1], s);
+    }
+    p = -1;
+    e = s = 0;
+  }
+  /* all threads of the block */
+  __device__ __forceinline__ void finish(double* sgrad, int n_params) {
+    flush_lj(sgrad);
+    const double t = warp_sum_dd(q);
+    if ((threadIdx.x & 31) == 0 && t != 0) atomicAdd(&sgrad[n_params - 1], t);
+    q = 0;
+  }
+};
+
 /* out += J_F(x)^T lam; grad += (dF/dtheta)^T lam.  Weights must be current. */
 __device__ void force_vjp(const Sys& S, const Buf& B, const double* x, const double* lam, double* out,
                           double* sgrad, const double* cent, double* red) {
   for (int i = threadIdx.x; i < S.N; i += blockDim.x) B.om[i] = 0;
   __syncthreads();
+  ParamSums ps;
   for (int p = threadIdx.x; p < S.n_pairs; p += blockDim.x) {
     const int i = S.pi[p], j = S.pj[p], k = S.pk[p];
     double d[3] = {x[3 * i] - x[3 * j], x[3 * i + 1] - x[3 * j + 1], x[3 * i + 2] - x[3 * j + 2]};
@@ -445,12 +486,10 @@ __device__ void force_vjp(const Sys& S, const Buf& B, const double* x, const dou
       if (S.vapor[i]) atomicAdd(&B.om[i], B.w[j] * t);
       if (S.vapor[j]) atomicAdd(&B.om[j], B.w[i] * t);
     }
-    if (e.ljp) {
-      atomicAdd(&sgrad[e.p], e.W * e.fe * dm);
-      atomicAdd(&sgrad[e.p + 1], e.W * e.fs_sig * dm);
-    }
-    if (e.fq != 0) atomicAdd(&sgrad[S.n_params - 1], e.W * e.fq * dm);
+    if (e.ljp) ps.add_lj(sgrad, e.p, e.W * e.fe * dm, e.W * e.fs_sig * dm);
+    if (e.fq != 0) ps.q += e.W * e.fq * dm;
   }
+  ps.finish(sgrad, S.n_params);
   __syncthreads();
   /* weights: x_i directly, and the ion centre c they are measured from */
   double s0 = 0, s1 = 0, s2 = 0;
@@ -509,6 +548,7 @@ __device__ void force_vjp(const Sys& S, const Buf& B, const double* x, const dou
 __device__ double objective(const Sys& S, const double* x, double* out, double* sgrad, const double* cent,
                             bool grad) {
   double jp = 0;
+  ParamSums ps;
   if (S.w_energy != 0)
     for (int p = threadIdx.x; p < S.n_pairs; p += blockDim.x) {
       if (S.pk[p] != PK_VI) continue;
@@ -528,12 +568,12 @@ __device__ double objective(const Sys& S, const double* x, double* out, double* 
         atomicAdd(&out[3 * j + q], -c * d[q]);
       }
       const int pb = S.pidx[tt];
-      if (pb >= 0) {
-        atomicAdd(&sgrad[pb], S.w_energy * S.inv_n * Ulj / S.eps[tt]);
-        atomicAdd(&sgrad[pb + 1], S.w_energy * S.inv_n * (S.A[tt] / (u3 * u3) - S.B[tt] / u3) / S.sig[tt]);
-      }
-      atomicAdd(&sgrad[S.n_params - 1], S.w_energy * S.inv_n * qq / r);
+      if (pb >= 0)
+        ps.add_lj(sgrad, pb, S.w_energy * S.inv_n * Ulj / S.eps[tt],
+                  S.w_energy * S.inv_n * (S.A[tt] / (u3 * u3) - S.B[tt] / u3) / S.sig[tt]);
+      ps.q += S.w_energy * S.inv_n * qq / r;
     }
+  if (grad) ps.finish(sgrad, S.n_params);
   if (S.w_count != 0)
     for (int m = threadIdx.x; m < S.n_vmol; m += blockDim.x) {
       const int a0 = S.vmol_first + m * S.a_v;
@@ -1105,6 +1145,24 @@ extern "C" int mdn_adjoint(mdn_handle* h, const mdn_replica_desc* d, const mdn_a
   S.mass = dput(mass, owned);
   S.c = dput(cc, owned);
   S.vapor = dput(isvap, owned);
+  /* pairs grouped by kind and type pair, so that a thread's strided run of
+   * pairs stays on one parameter row (ParamSums) */
+  {
+    std::vector<size_t> ord(pi.size());
+    for (size_t k = 0; k < ord.size(); k++) ord[k] = k;
+    auto key = [&](size_t k) { return ((long long)pk[k] * nt + type[pi[k]]) * nt + type[pj[k]]; };
+    std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return key(a) < key(b); });
+    std::vector<int> pi2(pi.size()), pj2(pi.size());
+    std::vector<unsigned char> pk2(pi.size());
+    for (size_t k = 0; k < ord.size(); k++) {
+      pi2[k] = pi[ord[k]];
+      pj2[k] = pj[ord[k]];
+      pk2[k] = pk[ord[k]];
+    }
+    pi.swap(pi2);
+    pj.swap(pj2);
+    pk.swap(pk2);
+  }
   S.n_pairs = (int)pi.size();
   S.pi = dput(pi, owned);
   S.pj = dput(pj, owned);
