@@ -24,6 +24,7 @@
  * Parameter derivatives accumulate in FP64 in shared memory; atomics make
  * sums independent of the launch shape up to FP64 rounding order.
  */
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdarg.h>
@@ -49,6 +50,7 @@ __attribute__((visibility("hidden"))) void mdn_snapshot_args(const mdn_handle* h
 namespace {
 
 constexpr int ADJ_THREADS = 512;
+constexpr int ADJ_CLUSTER = 8; /* CTAs of a reverse sweep (16 measured no faster) */
 constexpr int MAX_PARAMS = 512;
 constexpr int SHAKE_SWEEPS = 1000;
 
@@ -268,6 +270,56 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
   return s;
 }
 
+/* The reverse sweep runs on a cluster of CTAs: its loops are split over all
+ * the cluster's threads, its phases are separated by cluster barriers, and
+ * global data that other CTAs wrote in the same launch are read from L2
+ * (__ldcg), since the L1 caches are not coherent.  A kernel launched without
+ * a cluster is a cluster of one CTA (the recompute). */
+namespace cg = cooperative_groups;
+__device__ __forceinline__ int ctid() { return (int)(cg::this_cluster().block_rank() * blockDim.x + threadIdx.x); }
+__device__ __forceinline__ int cnthr() { return (int)(cg::this_cluster().num_blocks() * blockDim.x); }
+__device__ __forceinline__ void csync() {
+  cg::cluster_group cl = cg::this_cluster();
+  if (cl.num_blocks() > 1) {
+    __threadfence();
+    cl.sync();
+  } else {
+    __syncthreads();
+  }
+}
+
+/* three sums over the cluster at once, the same in every CTA (the CTAs'
+ * sums added in rank order; two cluster barriers) */
+__device__ void cluster_sum3(double* v, double* red) {
+  cg::cluster_group cl = cg::this_cluster();
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (l == 0)
+    for (int k = 0; k < 3; k++) red[4 * w + k] = v[k]; /* red holds >= 4 * 16 + 3 doubles */
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double t = 0;
+    for (int q = 0; q < nw; q++) t += red[4 * q + threadIdx.x];
+    red[64 + threadIdx.x] = t;
+  }
+  if (cl.num_blocks() > 1) {
+    cl.sync();
+    for (int k = 0; k < 3; k++) {
+      double t = 0;
+      for (unsigned r = 0; r < cl.num_blocks(); r++) t += *cl.map_shared_rank(&red[64 + k], r);
+      v[k] = t;
+    }
+    cl.sync();
+  } else {
+    __syncthreads();
+    for (int k = 0; k < 3; k++) v[k] = red[64 + k];
+    __syncthreads();
+  }
+}
+
 /* ion centre of x (mass-weighted) into cent[0..2] */
 __device__ void ion_centre(const Sys& S, const double* x, double* cent, double* red) {
   double sx = 0, sy = 0, sz = 0;
@@ -290,7 +342,7 @@ __device__ void ion_centre(const Sys& S, const double* x, double* cent, double* 
 /* taper weights and their gradients (src/verlet.cpp:109-134) */
 __device__ void weights(const Sys& S, const Buf& B, const double* x, const double* cent) {
   const double a = 3.141592653589793 / S.overlap * 0.5;
-  for (int i = threadIdx.x; i < S.N; i += blockDim.x) {
+  for (int i = ctid(); i < S.N; i += cnthr()) {
     double w = 1, g0 = 0, g1 = 0, g2 = 0;
     if (S.vapor[i]) {
       double dx = x[3 * i] - cent[0], dy = x[3 * i + 1] - cent[1], dz = x[3 * i + 2] - cent[2];
@@ -312,7 +364,7 @@ __device__ void weights(const Sys& S, const Buf& B, const double* x, const doubl
     B.dw[3 * i + 1] = g1;
     B.dw[3 * i + 2] = g2;
   }
-  __syncthreads();
+  /* no barrier: the callers' next barrier comes before any read */
 }
 
 /* force factor f(u) and df/du of one pair (u = r^2), parameter derivatives
@@ -365,7 +417,7 @@ __device__ __forceinline__ PairEval eval_pair(const Sys& S, const Buf& B, int i,
       if (kind == PK_VI) o.fq = fc;
       else if (kind == PK_ION_LJC) o.fq = 2.0 * fc;
     }
-    if (kind == PK_VI || kind == PK_VV) o.W = B.w[i] * B.w[j];
+    if (kind == PK_VI || kind == PK_VV) o.W = __ldcg(B.w + i) * __ldcg(B.w + j);
   }
   o.f = f;
   o.fp = fp;
@@ -466,15 +518,15 @@ struct ParamSums {
 /* out += J_F(x)^T lam; grad += (dF/dtheta)^T lam.  Weights must be current. */
 __device__ void force_vjp(const Sys& S, const Buf& B, const double* x, const double* lam, double* out,
                           double* sgrad, const double* cent, double* red) {
-  for (int i = threadIdx.x; i < S.N; i += blockDim.x) B.om[i] = 0;
-  __syncthreads();
+  /* B.om was zeroed before the caller's last cluster barrier */
   ParamSums ps;
-  for (int p = threadIdx.x; p < S.n_pairs; p += blockDim.x) {
+  for (int p = ctid(); p < S.n_pairs; p += cnthr()) {
     const int i = S.pi[p], j = S.pj[p], k = S.pk[p];
     double d[3] = {x[3 * i] - x[3 * j], x[3 * i + 1] - x[3 * j + 1], x[3 * i + 2] - x[3 * j + 2]};
     double u = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
     PairEval e = eval_pair(S, B, i, j, k, u);
-    double m[3] = {lam[3 * i] - lam[3 * j], lam[3 * i + 1] - lam[3 * j + 1], lam[3 * i + 2] - lam[3 * j + 2]};
+    double m[3] = {__ldcg(lam + 3 * i) - __ldcg(lam + 3 * j), __ldcg(lam + 3 * i + 1) - __ldcg(lam + 3 * j + 1),
+                   __ldcg(lam + 3 * i + 2) - __ldcg(lam + 3 * j + 2)};
     double dm = d[0] * m[0] + d[1] * m[1] + d[2] * m[2];
     for (int q = 0; q < 3; q++) {
       double g = e.W * (e.f * m[q] + 2.0 * e.fp * dm * d[q]);
@@ -483,40 +535,43 @@ __device__ void force_vjp(const Sys& S, const Buf& B, const double* x, const dou
     }
     if (k == PK_VI || k == PK_VV) {
       double t = e.f * dm;
-      if (S.vapor[i]) atomicAdd(&B.om[i], B.w[j] * t);
-      if (S.vapor[j]) atomicAdd(&B.om[j], B.w[i] * t);
+      if (S.vapor[i]) atomicAdd(&B.om[i], __ldcg(B.w + j) * t);
+      if (S.vapor[j]) atomicAdd(&B.om[j], __ldcg(B.w + i) * t);
     }
     if (e.ljp) ps.add_lj(sgrad, e.p, e.W * e.fe * dm, e.W * e.fs_sig * dm);
     if (e.fq != 0) ps.q += e.W * e.fq * dm;
   }
   ps.finish(sgrad, S.n_params);
-  __syncthreads();
+  csync();
   /* weights: x_i directly, and the ion centre c they are measured from */
   double s0 = 0, s1 = 0, s2 = 0;
-  for (int i = threadIdx.x; i < S.N; i += blockDim.x) {
+  for (int i = ctid(); i < S.N; i += cnthr()) {
     if (!S.vapor[i]) continue;
-    double o = B.om[i];
-    double g0 = o * B.dw[3 * i], g1 = o * B.dw[3 * i + 1], g2 = o * B.dw[3 * i + 2];
-    out[3 * i] += g0;
-    out[3 * i + 1] += g1;
-    out[3 * i + 2] += g2;
+    double o = __ldcg(B.om + i);
+    double g0 = o * __ldcg(B.dw + 3 * i), g1 = o * __ldcg(B.dw + 3 * i + 1), g2 = o * __ldcg(B.dw + 3 * i + 2);
+    atomicAdd(out + 3 * i, g0);
+    atomicAdd(out + 3 * i + 1, g1);
+    atomicAdd(out + 3 * i + 2, g2);
     s0 += g0;
     s1 += g1;
     s2 += g2;
   }
-  s0 = block_sum(s0, red);
-  s1 = block_sum(s1, red);
-  s2 = block_sum(s2, red);
-  for (int a = threadIdx.x; a < S.n_ion; a += blockDim.x) {
-    double fr = S.mass[a] / S.ion_msum;
-    out[3 * a] -= fr * s0;
-    out[3 * a + 1] -= fr * s1;
-    out[3 * a + 2] -= fr * s2;
+  {
+    double sv[3] = {s0, s1, s2};
+    cluster_sum3(sv, red);
+    s0 = sv[0];
+    s1 = sv[1];
+    s2 = sv[2];
   }
-  __syncthreads();
+  for (int a = ctid(); a < S.n_ion; a += cnthr()) {
+    double fr = S.mass[a] / S.ion_msum;
+    atomicAdd(out + 3 * a, -fr * s0);
+    atomicAdd(out + 3 * a + 1, -fr * s1);
+    atomicAdd(out + 3 * a + 2, -fr * s2);
+  }
   /* bonded terms: J lam by forward-mode products (symmetric Jacobians) */
   const int nb = S.n_bonds, na = S.n_angles, nd = S.n_dih;
-  for (int t = threadIdx.x; t < nb + na + nd; t += blockDim.x) {
+  for (int t = ctid(); t < nb + na + nd; t += cnthr()) {
     int at[4], n;
     Dual X[4][3], f[4][3];
     const int* r;
@@ -525,7 +580,7 @@ __device__ void force_vjp(const Sys& S, const Buf& B, const double* x, const dou
     else { r = S.dih + 5 * (t - nb - na); n = 4; }
     for (int a = 0; a < n; a++) {
       at[a] = r[a];
-      for (int k = 0; k < 3; k++) X[a][k] = mk(x[3 * at[a] + k], lam[3 * at[a] + k]);
+      for (int k = 0; k < 3; k++) X[a][k] = mk(x[3 * at[a] + k], __ldcg(lam + 3 * at[a] + k));
     }
     if (n == 2) bond_t<Dual>(X, S.bond_c + 2 * r[2], f);
     else if (n == 3) angle_t<Dual>(X, S.angle_c + 2 * r[3], f);
@@ -535,12 +590,15 @@ __device__ void force_vjp(const Sys& S, const Buf& B, const double* x, const dou
   }
   if (S.efield_on) {
     double sq = 0;
-    for (int i = threadIdx.x; i < S.n_ion; i += blockDim.x)
-      sq += 5.55e-5 * S.q[i] * (S.efield[0] * lam[3 * i] + S.efield[1] * lam[3 * i + 1] + S.efield[2] * lam[3 * i + 2]);
+    for (int i = ctid(); i < S.n_ion; i += cnthr())
+      sq += 5.55e-5 * S.q[i] *
+            (S.efield[0] * __ldcg(lam + 3 * i) + S.efield[1] * __ldcg(lam + 3 * i + 1) +
+             S.efield[2] * __ldcg(lam + 3 * i + 2));
+    /* this CTA's share; the CTAs' gradients are summed at the end */
     sq = block_sum(sq, red);
     if (threadIdx.x == 0) sgrad[S.n_params - 1] += sq;
   }
-  __syncthreads();
+  csync();
 }
 
 /* objective at x: value (returned by thread partial), gradient into out
@@ -550,7 +608,7 @@ __device__ double objective(const Sys& S, const double* x, double* out, double* 
   double jp = 0;
   ParamSums ps;
   if (S.w_energy != 0)
-    for (int p = threadIdx.x; p < S.n_pairs; p += blockDim.x) {
+    for (int p = ctid(); p < S.n_pairs; p += cnthr()) {
       if (S.pk[p] != PK_VI) continue;
       const int i = S.pi[p], j = S.pj[p];
       const int tt = S.type[i] * S.nt + S.type[j];
@@ -575,7 +633,7 @@ __device__ double objective(const Sys& S, const double* x, double* out, double* 
     }
   if (grad) ps.finish(sgrad, S.n_params);
   if (S.w_count != 0)
-    for (int m = threadIdx.x; m < S.n_vmol; m += blockDim.x) {
+    for (int m = ctid(); m < S.n_vmol; m += cnthr()) {
       const int a0 = S.vmol_first + m * S.a_v;
       double cm[3] = {0, 0, 0};
       for (int a = 0; a < S.a_v; a++)
@@ -596,7 +654,7 @@ __device__ double objective(const Sys& S, const double* x, double* out, double* 
         for (int q = 0; q < 3; q++) atomicAdd(&out[3 * b + q], -dSdrho * fr * dv[q] / rho);
       }
     }
-  __syncthreads();
+  /* no barrier: out is read only after the callers' next one */
   return jp;
 }
 
@@ -657,70 +715,76 @@ __device__ void shake(const Sys& S, const Buf& B, double* y, const double* xr, d
  * added into xb (adjoint of the reference positions xr) */
 __device__ void shake_adjoint(const Sys& S, const Buf& B, const double* x, const double* xr, const double* gam,
                               double* lam, double* xb) {
-  if (S.n_cons == 0) return;
-  /* G_{kl} = s_k . r_l * coef(k, l); G^T mu = rho, rho_l = r_l . (lam_i/m_i - lam_j/m_j) */
-  for (int k = threadIdx.x; k < S.n_cons; k += blockDim.x) B.mu[k] = 0;
-  __syncthreads();
-  auto G = [&](int k, int l) {
-    const int ik = S.cons[3 * k], jk = S.cons[3 * k + 1], il = S.cons[3 * l], jl = S.cons[3 * l + 1];
-    double coef = 0;
-    if (il == ik) coef += 1.0 / S.mass[il];
-    if (jl == ik) coef -= 1.0 / S.mass[jl];
-    if (il == jk) coef -= 1.0 / S.mass[il];
-    if (jl == jk) coef += 1.0 / S.mass[jl];
-    if (coef == 0) return 0.0;
-    double sr = 0;
-    for (int q = 0; q < 3; q++)
-      sr += (x[3 * ik + q] - x[3 * jk + q]) * (xr[3 * il + q] - xr[3 * jl + q]);
-    return sr * coef;
-  };
-  for (int sweep = 0; sweep < SHAKE_SWEEPS; sweep++) {
-    if (threadIdx.x == 0) B.flag[0] = 1;
+  /* the constraints are few: the first CTA of the cluster solves them with
+   * block barriers (x-bar, which the other CTAs added to, read from L2), the
+   * others wait at the cluster barrier below */
+  if (S.n_cons > 0 && cg::this_cluster().block_rank() == 0) {
+    /* G_{kl} = s_k . r_l * coef(k, l); G^T mu = rho, rho_l = r_l . (lam_i/m_i - lam_j/m_j) */
+    for (int k = (int)threadIdx.x; k < S.n_cons; k += (int)blockDim.x) B.mu[k] = 0;
     __syncthreads();
-    for (int col = 0; col < S.n_colors; col++) {
-      for (int l = threadIdx.x; l < S.n_cons; l += blockDim.x) {
-        if (S.cons_color[l] != col) continue;
-        const int il = S.cons[3 * l], jl = S.cons[3 * l + 1];
-        double rho = 0;
-        for (int q = 0; q < 3; q++) {
-          double rl = xr[3 * il + q] - xr[3 * jl + q];
-          rho += rl * (lam[3 * il + q] / S.mass[il] - lam[3 * jl + q] / S.mass[jl]);
-        }
-        double acc = rho;
-        for (int e = S.cons_nb_off[l]; e < S.cons_nb_off[l + 1]; e++) {
-          const int k = S.cons_nb[e];
-          acc -= G(k, l) * B.mu[k];
-        }
-        double nm = acc / G(l, l);
-        if (fabs(nm - B.mu[l]) > 1e-13 * (fabs(nm) + 1e-300)) B.flag[0] = 0;
-        B.mu[l] = nm;
-      }
+    auto G = [&](int k, int l) {
+      const int ik = S.cons[3 * k], jk = S.cons[3 * k + 1], il = S.cons[3 * l], jl = S.cons[3 * l + 1];
+      double coef = 0;
+      if (il == ik) coef += 1.0 / S.mass[il];
+      if (jl == ik) coef -= 1.0 / S.mass[jl];
+      if (il == jk) coef -= 1.0 / S.mass[il];
+      if (jl == jk) coef += 1.0 / S.mass[jl];
+      if (coef == 0) return 0.0;
+      double sr = 0;
+      for (int q = 0; q < 3; q++)
+        sr += (x[3 * ik + q] - x[3 * jk + q]) * (xr[3 * il + q] - xr[3 * jl + q]);
+      return sr * coef;
+    };
+    for (int sweep = 0; sweep < SHAKE_SWEEPS; sweep++) {
+      if ((int)threadIdx.x == 0) B.flag[0] = 1;
       __syncthreads();
+      for (int col = 0; col < S.n_colors; col++) {
+        for (int l = (int)threadIdx.x; l < S.n_cons; l += (int)blockDim.x) {
+          if (S.cons_color[l] != col) continue;
+          const int il = S.cons[3 * l], jl = S.cons[3 * l + 1];
+          double rho = 0;
+          for (int q = 0; q < 3; q++) {
+            double rl = xr[3 * il + q] - xr[3 * jl + q];
+            rho += rl * (__ldcg(lam + 3 * il + q) / S.mass[il] - __ldcg(lam + 3 * jl + q) / S.mass[jl]);
+          }
+          double acc = rho;
+          for (int e = S.cons_nb_off[l]; e < S.cons_nb_off[l + 1]; e++) {
+            const int k = S.cons_nb[e];
+            acc -= G(k, l) * B.mu[k];
+          }
+          double nm = acc / G(l, l);
+          if (fabs(nm - B.mu[l]) > 1e-13 * (fabs(nm) + 1e-300)) B.flag[0] = 0;
+          B.mu[l] = nm;
+        }
+        __syncthreads();
+      }
+      const int conv = B.flag[0];
+      __syncthreads();
+      if (conv) break;
     }
-    const int conv = B.flag[0];
+    /* lam_y = lam - sum_k mu_k B_k^T (B_k: +s_k at i_k, -s_k at j_k) */
+    for (int k = (int)threadIdx.x; k < S.n_cons; k += (int)blockDim.x) {
+      const int i = S.cons[3 * k], j = S.cons[3 * k + 1];
+      const double mk_ = B.mu[k];
+      for (int q = 0; q < 3; q++) {
+        double sk = x[3 * i + q] - x[3 * j + q];
+        atomicAdd(&lam[3 * i + q], -mk_ * sk);
+        atomicAdd(&lam[3 * j + q], mk_ * sk);
+      }
+    }
     __syncthreads();
-    if (conv) break;
-  }
-  /* lam_y = lam - sum_k mu_k B_k^T (B_k: +s_k at i_k, -s_k at j_k) */
-  for (int k = threadIdx.x; k < S.n_cons; k += blockDim.x) {
-    const int i = S.cons[3 * k], j = S.cons[3 * k + 1];
-    for (int q = 0; q < 3; q++) {
-      double sk = x[3 * i + q] - x[3 * j + q];
-      atomicAdd(&lam[3 * i + q], -B.mu[k] * sk);
-      atomicAdd(&lam[3 * j + q], B.mu[k] * sk);
+    /* g_l D_l dr_l: r_l = xr_i - xr_j */
+    for (int l = (int)threadIdx.x; l < S.n_cons; l += (int)blockDim.x) {
+      const int i = S.cons[3 * l], j = S.cons[3 * l + 1];
+      for (int q = 0; q < 3; q++) {
+        double t = gam[l] * (__ldcg(lam + 3 * i + q) / S.mass[i] - __ldcg(lam + 3 * j + q) / S.mass[j]);
+        atomicAdd(&xb[3 * i + q], t);
+        atomicAdd(&xb[3 * j + q], -t);
+      }
     }
+    __syncthreads();
   }
-  __syncthreads();
-  /* g_l D_l dr_l: r_l = xr_i - xr_j */
-  for (int l = threadIdx.x; l < S.n_cons; l += blockDim.x) {
-    const int i = S.cons[3 * l], j = S.cons[3 * l + 1];
-    for (int q = 0; q < 3; q++) {
-      double t = gam[l] * (lam[3 * i + q] / S.mass[i] - lam[3 * j + q] / S.mass[j]);
-      atomicAdd(&xb[3 * i + q], t);
-      atomicAdd(&xb[3 * j + q], -t);
-    }
-  }
-  __syncthreads();
+  csync();
 }
 
 /* The FP64 recompute of one segment: K steps from (X[0], V[0]), keeping x,
@@ -814,42 +878,46 @@ __global__ void __launch_bounds__(ADJ_THREADS, 1) adjoint_recompute(Sys S, Buf B
 __global__ void __launch_bounds__(ADJ_THREADS, 1) adjoint_segment(Sys S, Buf B, int K, int first,
                                                                   int f0_theta) {
   __shared__ double sgrad[MAX_PARAMS];
-  __shared__ double red[40];
+  __shared__ double red[72];
   __shared__ double cent[3];
   const int n3 = 3 * S.N;
   for (int p = threadIdx.x; p < S.n_params; p += blockDim.x) sgrad[p] = 0;
+  for (int i = ctid(); i < S.N; i += cnthr()) B.om[i] = 0;
   __syncthreads();
   for (int t = K; t >= 1; t--) {
     const double* x0 = B.X + (size_t)(t - 1) * n3;
     const double* x1 = B.X + (size_t)t * n3;
+    /* every CTA its own copy of the centre */
     ion_centre(S, x1, cent, red);
     weights(S, B, x1, cent);
     /* objective at x_t */
     objective(S, x1, B.lx, sgrad, cent, true);
-    /* (6): F-bar += c V-bar */
-    for (int q = threadIdx.x; q < n3; q += blockDim.x) B.lf[q] += S.c[q / 3] * B.lv[q];
-    __syncthreads();
+    /* (6): F-bar += c V-bar (each thread its own elements throughout) */
+    for (int q = ctid(); q < n3; q += cnthr()) B.lf[q] += S.c[q / 3] * B.lv[q];
+    csync();
     /* (5): x-bar += J^T F-bar */
     force_vjp(S, B, x1, B.lf, B.lx, sgrad, cent, red);
     /* (4): v_b = v_a + (x_t - y)/dt */
-    if (S.n_cons > 0 && S.vcorr)
-      for (int q = threadIdx.x; q < n3; q += blockDim.x) B.lx[q] += B.lv[q] / S.dt;
-    for (int q = threadIdx.x; q < n3; q += blockDim.x) B.xb[q] = 0;
-    __syncthreads();
+    const bool vc = S.n_cons > 0 && S.vcorr;
+    for (int q = ctid(); q < n3; q += cnthr()) {
+      if (vc) B.lx[q] = __ldcg(B.lx + q) + B.lv[q] / S.dt;
+      B.xb[q] = 0;
+    }
+    csync();
     /* (3): SHAKE adjoint: lx becomes the adjoint of y; xb gets the r-terms */
     if (S.n_cons > 0) shake_adjoint(S, B, x1, x0, B.gam + (size_t)(t - 1) * S.n_cons, B.lx, B.xb);
-    if (S.n_cons > 0 && S.vcorr)
-      for (int q = threadIdx.x; q < n3; q += blockDim.x) B.lx[q] -= B.lv[q] / S.dt;
-    __syncthreads();
     /* (2) y = x + dt v_a; (1) v_a = v + c F */
-    for (int q = threadIdx.x; q < n3; q += blockDim.x) {
-      const double ly = B.lx[q];
+    for (int q = ctid(); q < n3; q += cnthr()) {
+      double ly = __ldcg(B.lx + q);
+      if (vc) ly -= B.lv[q] / S.dt;
       const double lva = B.lv[q] + S.dt * ly;
-      B.lx[q] = ly + B.xb[q];
+      B.lx[q] = ly + __ldcg(B.xb + q);
       B.lv[q] = lva;
       B.lf[q] = S.c[q / 3] * lva;
     }
-    __syncthreads();
+    /* the weight adjoints of the next force product start at zero */
+    for (int i = ctid(); i < S.N; i += cnthr()) B.om[i] = 0;
+    csync();
   }
   if (first && f0_theta) {
     /* F(x_0): its parameter dependence */
@@ -858,7 +926,9 @@ __global__ void __launch_bounds__(ADJ_THREADS, 1) adjoint_segment(Sys S, Buf B, 
     force_vjp(S, B, B.X, B.lf, B.tmp, sgrad, cent, red);
   }
   __syncthreads();
-  for (int p = threadIdx.x; p < S.n_params; p += blockDim.x) B.grad[p] += sgrad[p];
+  /* the CTAs' shares of the gradient */
+  for (int p = threadIdx.x; p < S.n_params; p += blockDim.x)
+    if (sgrad[p] != 0) atomicAdd(B.grad + p, sgrad[p]);
 }
 
 /* ------------------------------------------------------------------------- */
@@ -1305,7 +1375,34 @@ extern "C" int mdn_adjoint(mdn_handle* h, const mdn_replica_desc* d, const mdn_a
     b.V += s * (K + 1) * n3;
     b.F += s * (K + 1) * n3;
     b.gam += (size_t)s * K * std::max(ncons, 1);
-    adjoint_segment<<<1, ADJ_THREADS, 0, stream>>>(S, b, n, s == 0 ? 1 : 0, f0_theta);
+    /* one cluster of ADJ_CLUSTER CTAs per segment (fewer if the GPU cannot
+     * place that many) */
+    cudaError_t le = cudaErrorUnknown;
+    if (ADJ_CLUSTER > 8) {
+      cudaFuncSetAttribute(adjoint_segment, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+      cudaGetLastError();
+    }
+    for (int C = ADJ_CLUSTER; C >= 1; C /= 2) {
+      cudaLaunchConfig_t cfg;
+      memset(&cfg, 0, sizeof cfg);
+      cfg.gridDim = dim3(C);
+      cfg.blockDim = dim3(ADJ_THREADS);
+      cfg.stream = stream;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = C;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      le = cudaLaunchKernelEx(&cfg, adjoint_segment, S, b, n, s == 0 ? 1 : 0, f0_theta);
+      if (le == cudaSuccess) break;
+      cudaGetLastError();
+    }
+    if (le != cudaSuccess) {
+      cleanup();
+      return err(MDN_ERR_CUDA, "mdn_adjoint: reverse sweep launch: %s", cudaGetErrorString(le));
+    }
   }
   cudaEventRecord(e1, stream);
   cudaError_t ce = cudaStreamSynchronize(stream);

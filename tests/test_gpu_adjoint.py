@@ -134,7 +134,11 @@ def test_torch_harness_returns_the_adjoint(eng):
     e = eng.Engine([spec], force_mode=1)
     J2, grad, _ = e.adjoint(**WINDOW)
     assert abs(J.item() - J2) <= 1e-12 * max(abs(J2), 1.0)
-    assert torch.allclose(theta.grad, torch.tensor(grad), rtol=1e-12, atol=0)
+    # the reverse sweep sums x-bar and the parameter rows with FP64 atomics
+    # from several CTAs, whose order varies from run to run: two runs agree
+    # to FP64 rounding of those sums, not bit for bit
+    g = torch.tensor(grad)
+    assert torch.allclose(theta.grad, g, rtol=1e-9, atol=1e-9 * float(g.abs().max()))
 
 
 CONFIG3_WINDOW = dict(n_steps=300, checkpoint_every=100, count_radius=10.0, count_width=1.0, w_energy=1.0,
