@@ -223,6 +223,7 @@ struct Sys {
   const int* cons_color;
   const int* cons_nb_off; /* CSR: constraints sharing an atom with constraint k */
   const int* cons_nb;
+  int n_cons_nb;          /* entries of cons_nb */
   double ri2, RI2, rcenter, overlap;
   double ion_msum, qqrd2e, dt;
   double efield[3];
@@ -290,6 +291,26 @@ __device__ __forceinline__ void csync() {
 
 /* three sums over the cluster at once, the same in every CTA (the CTAs'
  * sums added in rank order; two cluster barriers) */
+/* three sums over the block, the same in every thread; red >= 67 doubles */
+__device__ void block_sum3(double* v, double* red) {
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (l == 0)
+    for (int k = 0; k < 3; k++) red[4 * w + k] = v[k];
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double t = 0;
+    for (int q = 0; q < nw; q++) t += red[4 * q + threadIdx.x];
+    red[64 + threadIdx.x] = t;
+  }
+  __syncthreads();
+  for (int k = 0; k < 3; k++) v[k] = red[64 + k];
+  __syncthreads();
+}
+
 __device__ void cluster_sum3(double* v, double* red) {
   cg::cluster_group cl = cg::this_cluster();
 #pragma unroll
@@ -604,7 +625,7 @@ __device__ void force_vjp(const Sys& S, const Buf& B, const double* x, const dou
 /* objective at x: value (returned by thread partial), gradient into out
  * (scaled by inv_n) and parameter derivatives into sgrad */
 __device__ double objective(const Sys& S, const double* x, double* out, double* sgrad, const double* cent,
-                            bool grad) {
+                            bool grad, double* red) {
   double jp = 0;
   ParamSums ps;
   if (S.w_energy != 0)
@@ -632,8 +653,14 @@ __device__ double objective(const Sys& S, const double* x, double* out, double* 
       ps.q += S.w_energy * S.inv_n * qq / r;
     }
   if (grad) ps.finish(sgrad, S.n_params);
-  if (S.w_count != 0)
-    for (int m = ctid(); m < S.n_vmol; m += cnthr()) {
+  if (S.w_count != 0) {
+    /* every CTA takes every molecule (a handful); the first CTA adds the
+     * value and the vapor atoms' terms, and the ion atoms' shares of the
+     * centre's derivative are summed over the molecules first and then added
+     * once per ion atom, split over the cluster */
+    const bool lead = cg::this_cluster().block_rank() == 0;
+    double C[3] = {0, 0, 0};
+    for (int m = threadIdx.x; m < S.n_vmol; m += blockDim.x) {
       const int a0 = S.vmol_first + m * S.a_v;
       double cm[3] = {0, 0, 0};
       for (int a = 0; a < S.a_v; a++)
@@ -642,18 +669,24 @@ __device__ double objective(const Sys& S, const double* x, double* out, double* 
       double dv[3] = {cm[0] - cent[0], cm[1] - cent[1], cm[2] - cent[2]};
       double rho = sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
       double sgm = 1.0 / (1.0 + exp((rho - S.R0) / S.W));
-      jp += S.w_count * sgm;
+      if (lead) jp += S.w_count * sgm;
       if (!grad) continue;
       double dSdrho = -sgm * (1.0 - sgm) / S.W * S.w_count * S.inv_n;
-      for (int a = 0; a < S.a_v; a++) {
-        double fr = S.mass[a0 + a] / S.vmol_mass;
-        for (int q = 0; q < 3; q++) atomicAdd(&out[3 * (a0 + a) + q], dSdrho * fr * dv[q] / rho);
-      }
-      for (int b = 0; b < S.n_ion; b++) {
+      if (lead)
+        for (int a = 0; a < S.a_v; a++) {
+          double fr = S.mass[a0 + a] / S.vmol_mass;
+          for (int q = 0; q < 3; q++) atomicAdd(&out[3 * (a0 + a) + q], dSdrho * fr * dv[q] / rho);
+        }
+      for (int q = 0; q < 3; q++) C[q] += dSdrho * dv[q] / rho;
+    }
+    if (grad) {
+      block_sum3(C, red);
+      for (int b = ctid(); b < S.n_ion; b += cnthr()) {
         double fr = S.mass[b] / S.ion_msum;
-        for (int q = 0; q < 3; q++) atomicAdd(&out[3 * b + q], -dSdrho * fr * dv[q] / rho);
+        for (int q = 0; q < 3; q++) atomicAdd(&out[3 * b + q], -fr * C[q]);
       }
     }
+  }
   /* no barrier: out is read only after the callers' next one */
   return jp;
 }
@@ -714,7 +747,7 @@ __device__ void shake(const Sys& S, const Buf& B, double* y, const double* xr, d
  * lam (adjoint of x) -> lam_y written into lam, and the g_k D_k dr_k terms
  * added into xb (adjoint of the reference positions xr) */
 __device__ void shake_adjoint(const Sys& S, const Buf& B, const double* x, const double* xr, const double* gam,
-                              double* lam, double* xb) {
+                              double* lam, double* xb, double* sc) {
   /* the constraints are few: the first CTA of the cluster solves them with
    * block barriers (x-bar, which the other CTAs added to, read from L2), the
    * others wait at the cluster barrier below */
@@ -735,24 +768,32 @@ __device__ void shake_adjoint(const Sys& S, const Buf& B, const double* x, const
         sr += (x[3 * ik + q] - x[3 * jk + q]) * (xr[3 * il + q] - xr[3 * jl + q]);
       return sr * coef;
     };
+    /* what the sweeps reuse, once per step into shared memory (sc): rho_l,
+     * G_ll and G_kl of each neighbour entry */
+    double* const srho = sc;
+    double* const sdiag = sc + S.n_cons;
+    double* const snb = sc + 2 * S.n_cons;
+    for (int l = (int)threadIdx.x; l < S.n_cons; l += (int)blockDim.x) {
+      const int il = S.cons[3 * l], jl = S.cons[3 * l + 1];
+      double rho = 0;
+      for (int q = 0; q < 3; q++) {
+        double rl = xr[3 * il + q] - xr[3 * jl + q];
+        rho += rl * (__ldcg(lam + 3 * il + q) / S.mass[il] - __ldcg(lam + 3 * jl + q) / S.mass[jl]);
+      }
+      srho[l] = rho;
+      sdiag[l] = G(l, l);
+      for (int e = S.cons_nb_off[l]; e < S.cons_nb_off[l + 1]; e++) snb[e] = G(S.cons_nb[e], l);
+    }
+    __syncthreads();
     for (int sweep = 0; sweep < SHAKE_SWEEPS; sweep++) {
       if ((int)threadIdx.x == 0) B.flag[0] = 1;
       __syncthreads();
       for (int col = 0; col < S.n_colors; col++) {
         for (int l = (int)threadIdx.x; l < S.n_cons; l += (int)blockDim.x) {
           if (S.cons_color[l] != col) continue;
-          const int il = S.cons[3 * l], jl = S.cons[3 * l + 1];
-          double rho = 0;
-          for (int q = 0; q < 3; q++) {
-            double rl = xr[3 * il + q] - xr[3 * jl + q];
-            rho += rl * (__ldcg(lam + 3 * il + q) / S.mass[il] - __ldcg(lam + 3 * jl + q) / S.mass[jl]);
-          }
-          double acc = rho;
-          for (int e = S.cons_nb_off[l]; e < S.cons_nb_off[l + 1]; e++) {
-            const int k = S.cons_nb[e];
-            acc -= G(k, l) * B.mu[k];
-          }
-          double nm = acc / G(l, l);
+          double acc = srho[l];
+          for (int e = S.cons_nb_off[l]; e < S.cons_nb_off[l + 1]; e++) acc -= snb[e] * B.mu[S.cons_nb[e]];
+          double nm = acc / sdiag[l];
           if (fabs(nm - B.mu[l]) > 1e-13 * (fabs(nm) + 1e-300)) B.flag[0] = 0;
           B.mu[l] = nm;
         }
@@ -833,7 +874,7 @@ __device__ double recompute(const Sys& S, const Buf& B, int K, int first, const 
     forces(S, B, x1, f1);
     for (int q = threadIdx.x; q < n3; q += blockDim.x) v1[q] += S.c[q / 3] * f1[q];
     __syncthreads();
-    jacc += objective(S, x1, nullptr, nullptr, cent, false);
+    jacc += objective(S, x1, nullptr, nullptr, cent, false, red);
   }
   return block_sum(jacc, red);
 }
@@ -880,6 +921,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, 1) adjoint_segment(Sys S, Buf B, 
   __shared__ double sgrad[MAX_PARAMS];
   __shared__ double red[72];
   __shared__ double cent[3];
+  extern __shared__ double csh[]; /* 2 n_cons + n_cons_nb doubles for the SHAKE adjoint */
   const int n3 = 3 * S.N;
   for (int p = threadIdx.x; p < S.n_params; p += blockDim.x) sgrad[p] = 0;
   for (int i = ctid(); i < S.N; i += cnthr()) B.om[i] = 0;
@@ -891,7 +933,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, 1) adjoint_segment(Sys S, Buf B, 
     ion_centre(S, x1, cent, red);
     weights(S, B, x1, cent);
     /* objective at x_t */
-    objective(S, x1, B.lx, sgrad, cent, true);
+    objective(S, x1, B.lx, sgrad, cent, true, red);
     /* (6): F-bar += c V-bar (each thread its own elements throughout) */
     for (int q = ctid(); q < n3; q += cnthr()) B.lf[q] += S.c[q / 3] * B.lv[q];
     csync();
@@ -905,7 +947,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, 1) adjoint_segment(Sys S, Buf B, 
     }
     csync();
     /* (3): SHAKE adjoint: lx becomes the adjoint of y; xb gets the r-terms */
-    if (S.n_cons > 0) shake_adjoint(S, B, x1, x0, B.gam + (size_t)(t - 1) * S.n_cons, B.lx, B.xb);
+    if (S.n_cons > 0) shake_adjoint(S, B, x1, x0, B.gam + (size_t)(t - 1) * S.n_cons, B.lx, B.xb, csh);
     /* (2) y = x + dt v_a; (1) v_a = v + c F */
     for (int q = ctid(); q < n3; q += cnthr()) {
       double ly = __ldcg(B.lx + q);
@@ -1259,6 +1301,7 @@ extern "C" int mdn_adjoint(mdn_handle* h, const mdn_replica_desc* d, const mdn_a
   S.cons_color = dput(color, owned);
   S.cons_nb_off = dput(nboff, owned);
   S.cons_nb = dput(nb, owned);
+  S.n_cons_nb = (int)nb.size();
   S.ri2 = d->r_inter * d->r_inter;
   S.RI2 = (d->r_inter + d->overlap) * (d->r_inter + d->overlap);
   S.rcenter = d->r_inter - d->overlap * 0.5;
@@ -1363,6 +1406,16 @@ extern "C" int mdn_adjoint(mdn_handle* h, const mdn_replica_desc* d, const mdn_a
     }
   }
   /* ---- backward, one segment per launch, last first ---- */
+  const size_t cbytes = sizeof(double) * (2 * (size_t)ncons + (size_t)S.n_cons_nb);
+  if (cbytes > 200 * 1024) {
+    cleanup();
+    return err(MDN_ERR_CAPACITY, "mdn_adjoint: %d constraints in the domain, too many for the reverse sweep", ncons);
+  }
+  if (cbytes > 48 * 1024 &&
+      cudaFuncSetAttribute(adjoint_segment, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cbytes) != cudaSuccess) {
+    cleanup();
+    return err(MDN_ERR_CUDA, "mdn_adjoint: reverse sweep shared memory");
+  }
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -1387,6 +1440,7 @@ extern "C" int mdn_adjoint(mdn_handle* h, const mdn_replica_desc* d, const mdn_a
       memset(&cfg, 0, sizeof cfg);
       cfg.gridDim = dim3(C);
       cfg.blockDim = dim3(ADJ_THREADS);
+      cfg.dynamicSmemBytes = cbytes;
       cfg.stream = stream;
       cudaLaunchAttribute attr[1];
       attr[0].id = cudaLaunchAttributeClusterDimension;
