@@ -344,7 +344,10 @@ int  mdn_snapshot_noalloc(mdn_handle* h, long long* offset, long long capacity, 
  * the converged SHAKE projection with its velocity correction.  The window
  * must hold no effective-domain rebuild (the molecule set is fixed): a
  * window that would cross one is an error (raise Margin or shorten it).
- * Needs a handle with one replica and the thermostat off.               */
+ * Needs a handle with one replica and the thermostat off.  The recompute
+ * runs every segment at once; each reverse sweep runs on a cluster of up
+ * to 8 CTAs and sums with FP64 atomics, so two calls agree to FP64
+ * rounding of those sums, not bit for bit.                              */
 typedef struct mdn_adjoint_spec {
   long long n_steps;        /* window length                                  */
   int checkpoint_every;     /* K: steps per recomputed segment                */
